@@ -1,0 +1,468 @@
+"""Python host interface over the engine's C ABI (include/gsparc_b200.h).
+
+Mirrors the reference's SpTC interface for this path:
+
+* :func:`SpTC` is ``gsparc::SpTC`` (reference include/gsparc/sptc.cuh:16-26) with
+  the TensorManager steps that precede it in main.cu:293-321; its
+  ``dense_accumulator`` argument is the reference's ``-d`` (1 dense, 0 auto,
+  -1 ESC).
+* :func:`read_tns` is ``IOManager::ParseFromFile`` (include/gsparc/io_manager.tpp:24-34).
+* :func:`layout`, :func:`linearize`, :func:`sort_pairs`, :func:`index_match` are
+  the stage functions ``compute_nbtis/setup_slitom``, ``ConvertTensor``,
+  ``sort_64`` and ``IndexMatch``.
+
+Errors raise :class:`GsparcError` carrying the library's status code; the
+reference calls ``exit()`` instead.  There is no CPU fallback: the compiled
+library must be present (``python -m gsparc_b200.build``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .synth import CooTensor
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libgsparc_b200.so")
+CLI_PATH = os.path.join(_PKG, "bin", "gsparc")
+
+ACCUM_ESC, ACCUM_AUTO, ACCUM_DENSE = -1, 0, 1
+SINK_DISCARD, SINK_DEVICE, SINK_HOST = 0, 1, 2
+
+STATUS = {0: "ok", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "EIO", 5: "ETIMEOUT",
+          6: "EUNSUPPORTED", 7: "EINTERNAL", 8: "ECALLBACK"}
+
+
+class GsparcError(RuntimeError):
+    def __init__(self, status: int, what: str, msg: str):
+        super().__init__(f"{what}: {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class _Coo(ctypes.Structure):
+    _fields_ = [("order", ctypes.c_int), ("dims", ctypes.POINTER(ctypes.c_uint64)),
+                ("nnz", ctypes.c_uint64), ("idx", ctypes.POINTER(ctypes.c_void_p)),
+                ("val", ctypes.c_void_p), ("on_device", ctypes.c_int)]
+
+
+CHUNK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int)
+
+
+class _Sink(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("on_chunk", CHUNK_FN), ("user", ctypes.c_void_p),
+                ("host_keys", ctypes.c_void_p), ("host_vals", ctypes.c_void_p),
+                ("host_capacity", ctypes.c_uint64), ("max_chunk_nnz", ctypes.c_uint64)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("ir_nnz", ctypes.c_uint64), ("nnz", ctypes.c_uint64), ("nnz_x", ctypes.c_uint64),
+                ("nnz_y", ctypes.c_uint64), ("rows", ctypes.c_uint64), ("heavy_rows", ctypes.c_uint64),
+                ("chunks", ctypes.c_uint64), ("nbits_x", ctypes.c_int), ("nbits_y", ctypes.c_int),
+                ("ncbits", ctypes.c_int), ("nfbits_x", ctypes.c_int), ("nfbits_y", ctypes.c_int),
+                ("accumulator", ctypes.c_int), ("t_linearize_ms", ctypes.c_double),
+                ("t_sort_ms", ctypes.c_double), ("t_match_ms", ctypes.c_double),
+                ("t_plan_ms", ctypes.c_double), ("t_contract_ms", ctypes.c_double),
+                ("t_output_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
+                ("bytes_h2d", ctypes.c_uint64), ("bytes_d2h", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64), ("t_numeric_kernel_ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+EXPORTS = [
+    "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create",
+    "gsparc_ctx_destroy", "gsparc_ctx_memory", "gsparc_tensor_upload", "gsparc_tensor_free",
+    "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
+    "gsparc_free_host", "gsparc_layout", "gsparc_plan_shards", "gsparc_linearize",
+    "gsparc_sort_pairs", "gsparc_index_match", "gsparc_digest_chunk",
+]
+
+
+class Digest(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("key_hash", ctypes.c_uint64), ("unsorted", ctypes.c_uint64),
+                ("first_key", ctypes.c_uint64), ("last_key", ctypes.c_uint64),
+                ("val_sum", ctypes.c_double), ("val_abs_sum", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def lib():
+    """Load the compiled library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m gsparc_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, U64, I = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+    L.gsparc_version.restype = ctypes.c_char_p
+    L.gsparc_status_string.restype = ctypes.c_char_p
+    L.gsparc_status_string.argtypes = [I]
+    L.gsparc_last_error.restype = ctypes.c_char_p
+    L.gsparc_ctx_create.argtypes = [I, U64, ctypes.POINTER(P)]
+    L.gsparc_ctx_destroy.argtypes = [P]
+    L.gsparc_ctx_memory.argtypes = [P, P, P, P]
+    L.gsparc_tensor_upload.argtypes = [P, ctypes.POINTER(_Coo), P, ctypes.POINTER(P)]
+    L.gsparc_tensor_free.argtypes = [P, P]
+    L.gsparc_tensor_info.argtypes = [P, P, P, P]
+    L.gsparc_sptc.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(_Sink), ctypes.POINTER(Stats), P]
+    L.gsparc_sptc_shard.argtypes = [P, P, P, I, P, P, I, I, I, ctypes.POINTER(_Sink),
+                                    ctypes.POINTER(Stats), P]
+    L.gsparc_read_tns.argtypes = [ctypes.c_char_p, I, P, P, P, ctypes.POINTER(P), ctypes.POINTER(P)]
+    L.gsparc_write_tns.argtypes = [ctypes.c_char_p, I, U64, P, P]
+    L.gsparc_free_host.argtypes = [P]
+    L.gsparc_layout.argtypes = [I, P, I, P, P, P, P, P, P]
+    L.gsparc_plan_shards.argtypes = [P, U64, I, P]
+    L.gsparc_linearize.argtypes = [I, P, I, P, I, U64, P, P, P]
+    L.gsparc_sort_pairs.argtypes = [P, U64, P, P, I, P]
+    L.gsparc_index_match.argtypes = [P, U64, P, I, U64, P, I, P, P, P, P, P]
+    L.gsparc_digest_chunk.argtypes = [P, P, U64, ctypes.POINTER(Digest), P]
+    for name in EXPORTS:
+        getattr(L, name).restype = getattr(L, name).restype if name in (
+            "gsparc_version", "gsparc_status_string", "gsparc_last_error") else (
+            None if name == "gsparc_free_host" else ctypes.c_int)
+    _lib = L
+    return L
+
+
+def _check(st: int, what: str) -> None:
+    if st != 0:
+        msg = lib().gsparc_last_error().decode(errors="replace")
+        raise GsparcError(st, what, msg)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def version() -> str:
+    return lib().gsparc_version().decode()
+
+
+# ------------------------------------------------------------------ host helpers
+def layout(dims: Sequence[int], cmodes: Sequence[int]):
+    """(bits, shift, is_contract, ncbits, nfbits) of one operand."""
+    order = len(dims)
+    d = np.asarray(dims, np.uint64)
+    c = np.asarray(cmodes, np.int32)
+    bits = np.zeros(order, np.int32)
+    shift = np.zeros(order, np.int32)
+    isc = np.zeros(order, np.int32)
+    ncb = np.zeros(1, np.int32)
+    nfb = np.zeros(1, np.int32)
+    _check(lib().gsparc_layout(order, _p(d), len(c), _p(c), _p(bits), _p(shift), _p(isc),
+                               _p(ncb), _p(nfb)), "layout")
+    return bits, shift, isc.astype(bool), int(ncb[0]), int(nfb[0])
+
+
+def read_tns(path: str, nthreads: int = 0) -> CooTensor:
+    order = np.zeros(1, np.int32)
+    dims = np.zeros(32, np.uint64)
+    nnz = np.zeros(1, np.uint64)
+    pidx, pval = ctypes.c_void_p(), ctypes.c_void_p()
+    _check(lib().gsparc_read_tns(path.encode(), nthreads, _p(order), _p(dims), _p(nnz),
+                                 ctypes.byref(pidx), ctypes.byref(pval)), f"read_tns({path})")
+    o, n = int(order[0]), int(nnz[0])
+    try:
+        idx = np.ctypeslib.as_array(ctypes.cast(pidx, ctypes.POINTER(ctypes.c_uint64)),
+                                    shape=(max(o * n, 1),))[: o * n].reshape(o, n).copy()
+        val = np.ctypeslib.as_array(ctypes.cast(pval, ctypes.POINTER(ctypes.c_float)),
+                                    shape=(max(n, 1),))[:n].copy()
+    finally:
+        lib().gsparc_free_host(pidx)
+        lib().gsparc_free_host(pval)
+    return CooTensor([int(x) for x in dims[:o]], idx, val)
+
+
+def write_tns(path: str, idx: np.ndarray, val: np.ndarray) -> None:
+    idx = np.ascontiguousarray(idx, np.uint64)
+    val = np.ascontiguousarray(val, np.float32)
+    _check(lib().gsparc_write_tns(path.encode(), idx.shape[0], idx.shape[1], _p(idx), _p(val)),
+           f"write_tns({path})")
+
+
+def plan_shards(row_prod: np.ndarray, nshards: int) -> np.ndarray:
+    rp = np.ascontiguousarray(row_prod, np.uint64)
+    out = np.zeros(nshards + 1, np.uint64)
+    _check(lib().gsparc_plan_shards(_p(rp), rp.shape[0], nshards, _p(out)), "plan_shards")
+    return out
+
+
+# ------------------------------------------------------------------ engine
+class Context:
+    """One device and an HBM budget (replaces CudaMemoryPool, src/gsparc/cuda_memory.cpp:17-30)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._h = ctypes.c_void_p()
+        _check(lib().gsparc_ctx_create(device, hbm_budget, ctypes.byref(self._h)), "ctx_create")
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def memory(self):
+        a = np.zeros(3, np.uint64)
+        _check(lib().gsparc_ctx_memory(self._h, _p(a[0:1]), _p(a[1:2]), _p(a[2:3])), "ctx_memory")
+        return {"in_use": int(a[0]), "peak": int(a[1]), "budget": int(a[2])}
+
+    def close(self):
+        if self._h:
+            _check(lib().gsparc_ctx_destroy(self._h), "ctx_destroy")
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, t: CooTensor, stream: int = 0) -> "DeviceTensor":
+        return DeviceTensor(self, t, stream)
+
+
+class DeviceTensor:
+    """A COO tensor resident in the context's HBM budget."""
+
+    def __init__(self, ctx: Context, t, stream: int = 0):
+        self.ctx = ctx
+        self._h = ctypes.c_void_p()
+        order = len(t.dims)
+        self.dims = [int(d) for d in t.dims]
+        self._dims = np.asarray(self.dims, np.uint64)
+        on_device = 0
+        if isinstance(t, CooTensor):
+            self._idx = np.ascontiguousarray(t.idx, np.uint64)
+            self._val = np.ascontiguousarray(t.val, np.float32)
+            nnz = self._val.shape[0]
+            ptrs = [self._idx[m].ctypes.data for m in range(order)]
+            vptr = self._val.ctypes.data
+        else:  # (dims, idx_tensor[order, nnz] uint64/int64 cuda, val_tensor float32 cuda)
+            dims, idx, val = t.dims, t.idx, t.val
+            nnz = int(val.shape[0])
+            ptrs = [idx[m].data_ptr() for m in range(order)]
+            vptr = val.data_ptr()
+            on_device = 1 if idx.is_cuda else 0
+            self._keep = (idx, val)
+        arr = (ctypes.c_void_p * max(order, 1))(*ptrs)
+        coo = _Coo(order, self._dims.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), nnz, arr,
+                   vptr, on_device)
+        _check(lib().gsparc_tensor_upload(ctx.handle, ctypes.byref(coo), ctypes.c_void_p(stream),
+                                          ctypes.byref(self._h)), "tensor_upload")
+        self.nnz = nnz
+        self.order = order
+        self._idx = self._val = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def free(self):
+        if self._h:
+            _check(lib().gsparc_tensor_free(self.ctx.handle, self._h), "tensor_free")
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+@dataclass
+class SpTCResult:
+    nnz: int
+    ir_nnz: int
+    keys: Optional[np.ndarray]
+    vals: Optional[np.ndarray]
+    stats: dict = field(default_factory=dict)
+
+
+def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: Sequence[int],
+         dense_accumulator: int = ACCUM_AUTO, sink: str = "host", max_chunk_nnz: int = 0,
+         shard: int = 0, nshards: int = 1, stream: int = 0, on_chunk=None,
+         host_keys: Optional[np.ndarray] = None, host_vals: Optional[np.ndarray] = None) -> SpTCResult:
+    """Z = X x_{cx,cy} Y on resident operands.
+
+    sink: "host" (Z copied into numpy arrays), "discard" (computed chunk-wise
+    in HBM and dropped, like the reference), "device" (``on_chunk(keys_ptr,
+    vals_ptr, n, first)`` gets device pointers per chunk) or "ring" (chunks
+    stream through the given ``host_keys``/``host_vals`` arrays, ``on_chunk``
+    sees numpy views).
+    """
+    if len(cx) != len(cy):
+        raise ValueError("cx and cy must have the same length")
+    c1 = np.asarray(cx, np.int32)
+    c2 = np.asarray(cy, np.int32)
+    st = Stats()
+    s = _Sink()
+    s.max_chunk_nnz = max_chunk_nnz
+    keep = []
+    keys = vals = None
+    if sink == "discard":
+        s.kind = SINK_DISCARD
+    elif sink == "device":
+        if on_chunk is None:
+            raise ValueError("device sink needs on_chunk")
+        s.kind = SINK_DEVICE
+
+        def _cb(user, k, v, n, first, on_dev):
+            return int(bool(on_chunk(k, v, n, first)))
+        s.on_chunk = CHUNK_FN(_cb)
+        keep.append(s.on_chunk)
+    elif sink in ("host", "ring"):
+        s.kind = SINK_HOST
+        if sink == "host":
+            # exact size is known only after the symbolic pass: collect chunks
+            parts = []
+
+            def _cbh(user, k, v, n, first, on_dev):
+                if k == s.host_keys + 8 * first:
+                    return 0  # whole-Z mode: the chunk already sits at its final place
+                kk = np.ctypeslib.as_array(ctypes.cast(k, ctypes.POINTER(ctypes.c_uint64)), shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+                vv = np.ctypeslib.as_array(ctypes.cast(v, ctypes.POINTER(ctypes.c_float)), shape=(n,)).copy() if n else np.zeros(0, np.float32)
+                parts.append((first, kk, vv))
+                return 0
+            cap = 1 << 22
+            hk = np.zeros(cap, np.uint64) if host_keys is None else host_keys
+            hv = np.zeros(cap, np.float32) if host_vals is None else host_vals
+            s.host_keys = hk.ctypes.data
+            s.host_vals = hv.ctypes.data
+            s.host_capacity = min(hk.shape[0], hv.shape[0])
+            s.on_chunk = CHUNK_FN(_cbh)
+            keep += [s.on_chunk, hk, hv]
+        else:
+            if host_keys is None or host_vals is None:
+                raise ValueError("ring sink needs host_keys and host_vals")
+            s.host_keys = host_keys.ctypes.data
+            s.host_vals = host_vals.ctypes.data
+            s.host_capacity = min(host_keys.shape[0], host_vals.shape[0])
+            if on_chunk is not None:
+                def _cbr(user, k, v, n, first, on_dev):
+                    return int(bool(on_chunk(host_keys[:n], host_vals[:n], n, first)))
+                s.on_chunk = CHUNK_FN(_cbr)
+                keep.append(s.on_chunk)
+    else:
+        raise ValueError(f"unknown sink {sink!r}")
+    _check(lib().gsparc_sptc_shard(ctx.handle, X.handle, Y.handle, len(c1), _p(c1), _p(c2),
+                                   int(dense_accumulator), shard, nshards, ctypes.byref(s),
+                                   ctypes.byref(st), ctypes.c_void_p(stream)), "sptc")
+    if sink == "host":
+        parts.sort(key=lambda p: p[0])
+        if parts and st.nnz <= s.host_capacity:
+            # whole Z fits the staging arrays: chunks landed in order
+            keys = np.array(np.ctypeslib.as_array(ctypes.cast(s.host_keys, ctypes.POINTER(ctypes.c_uint64)), shape=(s.host_capacity,))[: st.nnz])
+            vals = np.array(np.ctypeslib.as_array(ctypes.cast(s.host_vals, ctypes.POINTER(ctypes.c_float)), shape=(s.host_capacity,))[: st.nnz])
+        else:
+            keys = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0, np.uint64)
+            vals = np.concatenate([p[2] for p in parts]) if parts else np.zeros(0, np.float32)
+    return SpTCResult(int(st.nnz), int(st.ir_nnz), keys, vals, st.as_dict())
+
+
+def SpTC(X: CooTensor, Y: CooTensor, cx: Sequence[int], cy: Sequence[int],
+         dense_accumulator: int = ACCUM_AUTO, device: int = 0, ctx: Optional[Context] = None,
+         **kw) -> SpTCResult:
+    """One-shot contraction of two host COO tensors (uploads, contracts, frees)."""
+    own = ctx is None
+    ctx = ctx or Context(device)
+    try:
+        dx = ctx.upload(X)
+        dy = dx if Y is X else ctx.upload(Y)
+        try:
+            return sptc(ctx, dx, dy, cx, cy, dense_accumulator, **kw)
+        finally:
+            dx.free()
+            if dy is not dx:
+                dy.free()
+    finally:
+        if own:
+            ctx.close()
+
+
+# ------------------------------------------------------------------ stage functions (torch device tensors)
+def linearize(dims, cmodes, role: int, idx_dev, stream: int = 0):
+    """Keys of one operand; idx_dev is a [order, nnz] int64/uint64 CUDA tensor."""
+    import torch
+    order, nnz = idx_dev.shape
+    d = np.asarray(dims, np.uint64)
+    c = np.asarray(cmodes, np.int32)
+    keys = torch.empty(nnz, dtype=torch.int64, device=idx_dev.device)
+    idx_dev = idx_dev.contiguous()
+    _check(lib().gsparc_linearize(order, _p(d), len(c), _p(c), role, nnz,
+                                  ctypes.c_void_p(idx_dev.data_ptr()), ctypes.c_void_p(keys.data_ptr()),
+                                  ctypes.c_void_p(stream)), "linearize")
+    return keys
+
+
+def sort_pairs(ctx: Context, keys, vals, nbits: int, stream: int = 0):
+    """In-place stable sort of CUDA tensors (int64 keys, float32 vals) by the low nbits."""
+    _check(lib().gsparc_sort_pairs(ctx.handle, keys.shape[0], ctypes.c_void_p(keys.data_ptr()),
+                                   ctypes.c_void_p(vals.data_ptr()), nbits, ctypes.c_void_p(stream)),
+           "sort_pairs")
+    return keys, vals
+
+
+def index_match(ctx: Context, xkeys, x_ncbits: int, ykeys, y_nfbits: int, stream: int = 0):
+    """(pos, cnt, prefix, ir) for sorted CUDA key tensors (int64)."""
+    import torch
+    nx = xkeys.shape[0]
+    dev = xkeys.device
+    pos = torch.zeros(nx, dtype=torch.int64, device=dev)
+    cnt = torch.zeros(nx, dtype=torch.int64, device=dev)
+    pre = torch.zeros(nx + 1, dtype=torch.int64, device=dev)
+    ir = np.zeros(1, np.uint64)
+    _check(lib().gsparc_index_match(ctx.handle, nx, ctypes.c_void_p(xkeys.data_ptr()), x_ncbits,
+                                    ykeys.shape[0], ctypes.c_void_p(ykeys.data_ptr()), y_nfbits,
+                                    ctypes.c_void_p(pos.data_ptr()), ctypes.c_void_p(cnt.data_ptr()),
+                                    ctypes.c_void_p(pre.data_ptr()), _p(ir), ctypes.c_void_p(stream)),
+           "index_match")
+    return pos, cnt, pre, int(ir[0])
+
+
+def digest_chunk(keys_ptr: int, vals_ptr: int, n: int, stream: int = 0) -> dict:
+    """Verification digest of n output nonzeros at device pointers."""
+    d = Digest()
+    _check(lib().gsparc_digest_chunk(ctypes.c_void_p(keys_ptr), ctypes.c_void_p(vals_ptr), n,
+                                     ctypes.byref(d), ctypes.c_void_p(stream)), "digest_chunk")
+    return d.as_dict()
+
+
+def splitmix64(k: np.ndarray) -> np.ndarray:
+    """Host twin of the digest's key mix (mod 2^64)."""
+    with np.errstate(over="ignore"):
+        x = np.asarray(k, np.uint64) + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return x ^ (x >> np.uint64(31))
+
+
+def decode_keys(keys: np.ndarray, x_dims, y_dims, cx, cy) -> np.ndarray:
+    """Output keys -> coordinates [X free modes ascending, Y free modes ascending]."""
+    bx, sx, icx, ncx, nfx = layout(x_dims, cx)
+    by, sy, icy, ncy, nfy = layout(y_dims, cy)
+    k = np.asarray(keys, np.uint64)
+    xf = k >> np.uint64(nfy) if nfy < 64 else np.zeros_like(k)
+    yf = k & np.uint64((1 << nfy) - 1) if nfy < 64 else k
+    cols = []
+    for m in range(len(x_dims)):
+        if not icx[m]:
+            cols.append((xf >> np.uint64(sx[m])) & np.uint64((1 << int(bx[m])) - 1))
+    for m in range(len(y_dims)):
+        if not icy[m]:
+            cols.append((yf >> np.uint64(sy[m])) & np.uint64((1 << int(by[m])) - 1))
+    return np.stack(cols) if cols else np.zeros((0, k.shape[0]), np.uint64)

@@ -1,0 +1,271 @@
+// cli.cpp -- the `gsparc` command line, a thin program over the C ABI.
+//
+// Same options and stderr report as the reference binary
+// (reference: src/gsparc/cmdline_opts.cpp:9-193, main.cu:22-437):
+//   gsparc -X x.tns -Y y.tns -c N -x m1 .. mN -y m1 .. mN [-g G] [-n iters] [-d 1|0|-1]
+// Extension: -o z.tns writes the output tensor (1-based, %.9g values).
+// Not supported here (they are separate features of the reference): -q
+// (quantum directory input) and -m/-a/-z (chained multi-SpTC).
+#include <getopt.h>
+
+#include <chrono>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "gsparc_b200.h"
+
+namespace {
+
+struct Opts {
+    std::string X, Y, out;
+    int nc = 0;
+    std::vector<int> cx, cy;
+    int gpus = 1, iters = 1, dense = 0;
+    bool quantum = false;
+    int multi = 0;
+};
+
+[[noreturn]] void die(const char *what, gsparc_status st) {
+    std::fprintf(stderr, "gsparc: %s: %s (%s)\n", what, gsparc_status_string(st), gsparc_last_error());
+    std::exit(1);
+}
+
+void usage(const char *argv0) {
+    std::fprintf(stderr,
+                 "Usage: %s -X x.tns -Y y.tns -c N -x m1..mN -y m1..mN [-g G] [-n iters] [-d 1|0|-1] [-o z.tns]\n",
+                 argv0);
+}
+
+struct Tensor {
+    int order = 0;
+    uint64_t dims[32] = {};
+    uint64_t nnz = 0;
+    uint64_t *idx = nullptr;
+    float *val = nullptr;
+};
+
+struct OutCollect {
+    std::vector<uint64_t> keys;
+    std::vector<float> vals;
+};
+
+int collect_chunk(void *user, const uint64_t *k, const float *v, uint64_t n, uint64_t first, int on_device) {
+    (void)on_device;
+    auto *c = static_cast<OutCollect *>(user);
+    if (c->keys.size() < first + n) {
+        c->keys.resize(first + n);
+        c->vals.resize(first + n);
+    }
+    std::memcpy(c->keys.data() + first, k, 8 * n);
+    std::memcpy(c->vals.data() + first, v, 4 * n);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    Opts o;
+    int c;
+    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhv")) != -1) {
+        switch (c) {
+        case 'X':
+            std::fprintf(stderr, "tensor X: %s\n", optarg);
+            o.X = optarg;
+            break;
+        case 'Y':
+            std::fprintf(stderr, "tensor Y: %s\n", optarg);
+            o.Y = optarg;
+            break;
+        case 'c':
+            o.nc = std::atoi(optarg);
+            break;
+        case 'x':
+        case 'y': {
+            // the modes follow the flag as separate arguments (cmdline_opts.cpp:112-139)
+            std::vector<int> &v = c == 'x' ? o.cx : o.cy;
+            std::fprintf(stderr, "# contract modes of %c: %d, contract modes: ", c == 'x' ? 'X' : 'Y', o.nc);
+            v.clear();
+            for (int i = 0; i < o.nc; ++i) {
+                if (optind - 1 + i >= argc) {
+                    std::fprintf(stderr, "\ngsparc: -%c needs %d modes\n", c, o.nc);
+                    return 1;
+                }
+                v.push_back(std::atoi(argv[optind - 1 + i]));
+                std::fprintf(stderr, "%d ", v.back());
+            }
+            std::fprintf(stderr, "\n");
+            optind += o.nc - 1;
+            break;
+        }
+        case 'g':
+            o.gpus = std::atoi(optarg);
+            std::fprintf(stderr, "num_gpus: %d\n", o.gpus);
+            break;
+        case 'n':
+            o.iters = std::atoi(optarg);
+            break;
+        case 'd':
+            o.dense = std::atoi(optarg);
+            std::fprintf(stderr, "dense_accumulator: %d\n", o.dense);
+            break;
+        case 'o':
+            o.out = optarg;
+            break;
+        case 'q':
+            o.quantum = true;
+            break;
+        case 'm':
+            o.multi = std::atoi(optarg);
+            break;
+        case 'a':
+        case 'z':
+        case 'b':
+        case 'v':
+            break;
+        case 'h':
+            usage(argv[0]);
+            return 0;
+        default:
+            usage(argv[0]);
+            return 1;
+        }
+    }
+    if (o.quantum) {
+        std::fprintf(stderr, "gsparc: the quantum input format (-q) is not supported by this build\n");
+        return 1;
+    }
+    if (o.multi) {
+        std::fprintf(stderr, "gsparc: chained multi-SpTC (-m) is not supported by this build\n");
+        return 1;
+    }
+    if (o.X.empty() || o.Y.empty() || o.nc < 1 || (int)o.cx.size() != o.nc || (int)o.cy.size() != o.nc ||
+        o.gpus < 1 || o.iters < 1 || o.dense < -1 || o.dense > 1) {
+        usage(argv[0]);
+        return 1;
+    }
+
+    Tensor tx, ty;
+    gsparc_status st = gsparc_read_tns(o.X.c_str(), 0, &tx.order, tx.dims, &tx.nnz, &tx.idx, &tx.val);
+    if (st) die("reading X", st);
+    st = gsparc_read_tns(o.Y.c_str(), 0, &ty.order, ty.dims, &ty.nnz, &ty.idx, &ty.val);
+    if (st) die("reading Y", st);
+
+    double slitom = 0, idxmatch = 0, contraction = 0, dprtn = 0;
+    uint64_t result_nnz = 0;
+    OutCollect out;
+
+    for (int it = 0; it < o.iters; ++it) {
+        std::vector<gsparc_stats> stats(o.gpus);
+        std::vector<gsparc_status> sts(o.gpus, GSPARC_OK);
+        std::vector<double> upload_ms(o.gpus, 0.0);
+        std::vector<OutCollect> parts(o.gpus);
+        auto run = [&](int g) {
+            gsparc_ctx *ctx = nullptr;
+            gsparc_status s = gsparc_ctx_create(g, 0, &ctx);
+            if (s) { sts[g] = s; return; }
+            const uint64_t *ix[32], *iy[32];
+            for (int m = 0; m < tx.order; ++m) ix[m] = tx.idx + (size_t)m * tx.nnz;
+            for (int m = 0; m < ty.order; ++m) iy[m] = ty.idx + (size_t)m * ty.nnz;
+            gsparc_coo cx{tx.order, tx.dims, tx.nnz, ix, tx.val, 0};
+            gsparc_coo cy{ty.order, ty.dims, ty.nnz, iy, ty.val, 0};
+            gsparc_tensor *X = nullptr, *Y = nullptr;
+            auto t0 = std::chrono::steady_clock::now();
+            if (!(s = gsparc_tensor_upload(ctx, &cx, nullptr, &X)) &&
+                !(s = gsparc_tensor_upload(ctx, &cy, nullptr, &Y))) {
+                upload_ms[g] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                gsparc_sink sink{};
+                sink.kind = o.out.empty() ? GSPARC_SINK_DISCARD : GSPARC_SINK_DEVICE;
+                std::vector<uint64_t> hk;
+                std::vector<float> hv;
+                if (!o.out.empty()) {
+                    sink.kind = GSPARC_SINK_HOST;
+                    hk.resize(1 << 24);
+                    hv.resize(1 << 24);
+                    sink.host_keys = hk.data();
+                    sink.host_vals = hv.data();
+                    sink.host_capacity = hk.size();
+                    sink.on_chunk = collect_chunk;
+                    sink.user = &parts[g];
+                }
+                s = gsparc_sptc_shard(ctx, X, Y, o.nc, o.cx.data(), o.cy.data(), o.dense, g, o.gpus, &sink,
+                                      &stats[g], nullptr);
+            }
+            if (X) gsparc_tensor_free(ctx, X);
+            if (Y) gsparc_tensor_free(ctx, Y);
+            gsparc_ctx_destroy(ctx);
+            sts[g] = s;
+        };
+        std::vector<std::thread> th;
+        for (int g = 0; g < o.gpus; ++g) th.emplace_back(run, g);
+        for (auto &t : th) t.join();
+        for (int g = 0; g < o.gpus; ++g)
+            if (sts[g]) die("contraction", sts[g]);
+        for (int g = 0; g < o.gpus; ++g) {
+            const gsparc_stats &s = stats[g];
+            if (s.accumulator == GSPARC_ACCUM_DENSE) std::fprintf(stderr, "Dense Accumulator\n");
+            result_nnz += s.nnz;
+            slitom += (upload_ms[g] + s.t_linearize_ms + s.t_sort_ms) / 1e3 / o.gpus;
+            idxmatch += s.t_match_ms / 1e3 / o.gpus;
+            dprtn += s.t_plan_ms / 1e3 / o.gpus;
+            contraction += s.t_contract_ms / 1e3 / o.gpus;
+        }
+        if (it == 0 && !o.out.empty()) {
+            uint64_t base = 0;
+            for (int g = 0; g < o.gpus; ++g) {
+                out.keys.insert(out.keys.end(), parts[g].keys.begin(), parts[g].keys.end());
+                out.vals.insert(out.vals.end(), parts[g].vals.begin(), parts[g].vals.end());
+                base += parts[g].keys.size();
+            }
+        }
+    }
+
+    const double partition = 0.0;
+    const double n = o.iters;
+    const double total = slitom + partition + idxmatch + contraction + dprtn;
+    std::fprintf(stderr, "--------Break Down--------\n");
+    std::fprintf(stderr, "SLITOM time: %f\n", slitom / n);
+    std::fprintf(stderr, "Partition time: %f\n", partition / n);
+    std::fprintf(stderr, "Idxmatch time: %f\n", idxmatch / n);
+    std::fprintf(stderr, "Contraction time: %f\n", contraction / n);
+    std::fprintf(stderr, "Dynamic Partition time: %f\n", dprtn / n);
+    std::fprintf(stderr, "--------Elapsed Time--------\n");
+    std::fprintf(stderr, "Result NNZ: %llu\n", (unsigned long long)(result_nnz / o.iters));
+    std::fprintf(stderr, "SLITOM time: %f\n", slitom / n);
+    std::fprintf(stderr, "Partition time: %f\n", partition / n);
+    std::fprintf(stderr, "SpTC(IdxMatch + Contraction + Data Copy) time: %f\n", (idxmatch + contraction + dprtn) / n);
+    std::fprintf(stderr, "Total time: %f\n", total / n);
+    std::fprintf(stderr, "\n\n");
+
+    if (!o.out.empty()) {
+        // decode keys into coordinates: X free modes ascending, then Y free modes
+        int bx[32], shx[32], icx[32], ncx, nfx, by[32], shy[32], icy[32], ncy, nfy;
+        gsparc_layout(tx.order, tx.dims, o.nc, o.cx.data(), bx, shx, icx, &ncx, &nfx);
+        gsparc_layout(ty.order, ty.dims, o.nc, o.cy.data(), by, shy, icy, &ncy, &nfy);
+        std::vector<int> fmx, fmy;
+        for (int m = 0; m < tx.order; ++m) if (!icx[m]) fmx.push_back(m);
+        for (int m = 0; m < ty.order; ++m) if (!icy[m]) fmy.push_back(m);
+        const int zo = (int)(fmx.size() + fmy.size());
+        const uint64_t zn = out.keys.size();
+        std::vector<uint64_t> zi((size_t)zo * zn);
+        for (uint64_t k = 0; k < zn; ++k) {
+            uint64_t key = out.keys[k];
+            uint64_t xf = nfy >= 64 ? 0 : key >> nfy;
+            uint64_t yf = nfy >= 64 ? key : key & ((1ull << nfy) - 1);
+            int z = 0;
+            for (int m : fmx) zi[(size_t)(z++) * zn + k] = (xf >> shx[m]) & ((bx[m] >= 64) ? ~0ull : ((1ull << bx[m]) - 1));
+            for (int m : fmy) zi[(size_t)(z++) * zn + k] = (yf >> shy[m]) & ((by[m] >= 64) ? ~0ull : ((1ull << by[m]) - 1));
+        }
+        st = gsparc_write_tns(o.out.c_str(), zo, zn, zi.data(), out.vals.data());
+        if (st) die("writing Z", st);
+    }
+    gsparc_free_host(tx.idx);
+    gsparc_free_host(tx.val);
+    gsparc_free_host(ty.idx);
+    gsparc_free_host(ty.val);
+    return 0;
+}

@@ -1,0 +1,21 @@
+// engine.h -- entry points of the contraction engine (C++ side of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace gs {
+
+void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int nc, const int *cx,
+          const int *cy, int accum, int shard, int nshards, const gsparc_sink *sink,
+          gsparc_stats *st, cudaStream_t s);
+
+void plan_shards(const uint64_t *row_prod, uint64_t nrows, int nshards, uint64_t *bounds);
+
+// .tns text I/O (tns_io.cpp)
+void read_tns(const char *path, int nthreads, int *order, uint64_t *dims, uint64_t *nnz,
+              uint64_t **idx, float **val);
+void write_tns(const char *path, int order, uint64_t nnz, const uint64_t *idx, const float *val);
+
+}  // namespace gs

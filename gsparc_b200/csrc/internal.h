@@ -1,0 +1,140 @@
+// internal.h -- host-side internals shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "gsparc_b200.h"
+
+namespace gs {
+
+constexpr int kMaxOrder = 32;
+
+// Errors travel as exceptions inside the library and become status codes at
+// the C ABI boundary (capi.cpp).
+struct Error {
+    gsparc_status st;
+    std::string msg;
+};
+
+[[noreturn]] void fail(gsparc_status st, const std::string &msg);
+// Count of this library's own kernel launches (process-wide).
+void count_launch(uint64_t n = 1);
+uint64_t launch_count();
+void set_last_error(const std::string &msg);
+const char *last_error();
+
+#define GS_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            ::gs::fail(GSPARC_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define GS_REQUIRE(cond, st, msg)        \
+    do {                                 \
+        if (!(cond))                     \
+            ::gs::fail((st), (msg));     \
+    } while (0)
+
+// Bit layout of one operand (reference: include/gsparc/tensor_manager.tpp:91-210).
+struct Layout {
+    int order = 0;
+    int nc = 0;
+    int bits[kMaxOrder] = {};
+    int shift[kMaxOrder] = {};
+    int is_c[kMaxOrder] = {};
+    int cpos[kMaxOrder] = {};
+    int ncbits = 0;
+    int nfbits = 0;
+    int nbits() const { return ncbits + nfbits; }
+};
+
+int mode_bits(uint64_t dim);
+Layout make_layout(int order, const uint64_t *dims, int nc, const int *cmodes);
+
+// Device memory admitted against a byte budget.  Backed by a private
+// stream-ordered memory pool, so freeing a buffer on the stream that used it
+// makes it reusable by later work on that stream without a device sync.
+// (Replaces the reference's first-fit CudaMemoryPool, which grabbed all free
+// HBM minus 256 MiB and exited on exhaustion: src/gsparc/cuda_memory.cpp:17-80.)
+class Arena {
+public:
+    Arena() = default;
+    ~Arena();
+    void init(int device, uint64_t budget);
+    void *alloc(size_t bytes, cudaStream_t s);
+    void free(void *p, cudaStream_t s);
+    uint64_t in_use() const { return in_use_; }
+    uint64_t peak() const { return peak_; }
+    uint64_t budget() const { return budget_; }
+    uint64_t available() const { return budget_ > in_use_ ? budget_ - in_use_ : 0; }
+    int device() const { return device_; }
+
+private:
+    int device_ = -1;
+    cudaMemPool_t pool_ = nullptr;
+    uint64_t budget_ = 0, in_use_ = 0, peak_ = 0;
+    std::unordered_map<void *, size_t> sizes_;
+};
+
+// RAII device buffer from an Arena.
+template <class T>
+class DBuf {
+public:
+    DBuf() = default;
+    DBuf(Arena &a, size_t n, cudaStream_t s) { reset(a, n, s); }
+    ~DBuf() { release(); }
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    DBuf(DBuf &&o) noexcept { *this = std::move(o); }
+    DBuf &operator=(DBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            a_ = o.a_; p_ = o.p_; n_ = o.n_; s_ = o.s_;
+            o.a_ = nullptr; o.p_ = nullptr; o.n_ = 0;
+        }
+        return *this;
+    }
+    void reset(Arena &a, size_t n, cudaStream_t s) {
+        release();
+        a_ = &a; s_ = s; n_ = n;
+        p_ = static_cast<T *>(a.alloc(sizeof(T) * (n ? n : 1), s));
+    }
+    void release() {
+        if (a_ && p_) a_->free(p_, s_);
+        a_ = nullptr; p_ = nullptr; n_ = 0;
+    }
+    T *get() const { return p_; }
+    size_t size() const { return n_; }
+    operator T *() const { return p_; }
+
+private:
+    Arena *a_ = nullptr;
+    T *p_ = nullptr;
+    size_t n_ = 0;
+    cudaStream_t s_ = nullptr;
+};
+
+}  // namespace gs
+
+struct gsparc_ctx {
+    int device = 0;
+    gs::Arena arena;
+    int sm_count = 148;
+    cudaEvent_t ev[16] = {};
+    unsigned int *d_flag = nullptr;  // device error / work counters
+};
+
+struct gsparc_tensor {
+    int order = 0;
+    uint64_t dims[gs::kMaxOrder] = {};
+    uint64_t nnz = 0;
+    uint64_t *d_idx = nullptr;  // SoA, order * nnz
+    float *d_val = nullptr;
+    bool owned = true;
+};

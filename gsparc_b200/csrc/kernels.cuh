@@ -1,0 +1,114 @@
+// kernels.cuh -- launch interfaces of the engine's device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "internal.h"
+
+namespace gs {
+
+// ---- linearise (reference: include/gsparc/tensor_manager.tpp:246-294) ----
+struct LinParams {
+    int order;
+    int role;       // 0: X layout f<<ncbits|c, 1: Y layout c<<nfbits|f
+    int ncbits, nfbits;
+    int shift[kMaxOrder];
+    int is_c[kMaxOrder];
+    uint64_t dims[kMaxOrder];
+};
+LinParams make_lin_params(const Layout &L, const uint64_t *dims, int role);
+// keys[k] from SoA idx (idx[m*nnz+k]); optionally copies val -> val_out.
+// Out-of-range indices set bit 0 of *err.
+void launch_linearize(const LinParams &p, uint64_t nnz, const uint64_t *idx, const float *val,
+                      uint64_t *keys, float *val_out, unsigned int *err, cudaStream_t s);
+
+// ---- sort (CUB radix sort; reference: include/gsparc/sort.cuh:90-108) ----
+// Sorts (keys, vals) by bits [0, nbits).  keys/vals are double buffers: on
+// return *which tells which of the two holds the result (0 or 1).
+void sort_pairs(Arena &a, uint64_t n, uint64_t *keys0, uint64_t *keys1, float *vals0, float *vals1,
+                int nbits, int *which, cudaStream_t s);
+void sort_keys(Arena &a, uint64_t n, uint64_t *keys0, uint64_t *keys1, int nbits, int *which,
+               cudaStream_t s);
+
+// ---- Y preparation ----
+// From sorted Y keys (c << nfbits | f): per-entry column rank among the
+// distinct free indices, the distinct free indices, and the run table of
+// contract keys (run r covers [run_start[r], run_start[r+1])).
+struct YPrep {
+    uint64_t ny = 0, ncols = 0, nruns = 0;
+    DBuf<uint32_t> rank;      // [ny]
+    DBuf<uint64_t> cols;      // [ncols] distinct y_f ascending
+    DBuf<uint64_t> run_key;   // [nruns]
+    DBuf<uint32_t> run_start; // [nruns+1]
+};
+void prepare_y(Arena &a, const uint64_t *ykeys, uint64_t ny, int y_nfbits, YPrep &out,
+               cudaStream_t s);
+
+// ---- X match + rows ----
+struct XMatch {
+    uint64_t nx = 0, nrows = 0, ir = 0;
+    DBuf<uint32_t> pos;        // [nx] first Y index of the matching run
+    DBuf<uint32_t> cnt;        // [nx] run length (0: no match)
+    DBuf<uint64_t> xprefix;    // [nx+1] exclusive prefix of cnt
+    DBuf<uint32_t> row_start;  // [nrows+1]
+    DBuf<uint64_t> row_xf;     // [nrows]
+    DBuf<uint64_t> row_prod;   // [nrows]
+};
+void match_x(Arena &a, const uint64_t *xkeys, uint64_t nx, int x_ncbits, const YPrep &y,
+             XMatch &out, cudaStream_t s);
+
+// ---- accumulation ----
+struct AccArgs {
+    // X side
+    const uint32_t *row_start;
+    const uint64_t *row_xf;
+    const uint32_t *pos;
+    const uint32_t *cnt;
+    const uint64_t *xprefix;
+    const float *xval;
+    // Y side
+    const uint32_t *yrank;
+    const float *yval;
+    const uint64_t *cols;
+    int y_nfbits;
+    // work
+    const uint32_t *units;     // light: pairs (r0, r1); heavy: row ids
+    uint32_t nunits;
+    unsigned int *work_counter;
+    uint32_t *cursor;          // [nx] scratch (heavy path)
+    // symbolic output
+    uint32_t *row_nnz;         // [nrows]
+    // numeric output
+    const uint64_t *row_off;   // [nrows] exclusive prefix of row_nnz
+    uint64_t chunk_base;
+    uint64_t *out_keys;
+    float *out_vals;
+    unsigned int *err;
+};
+
+constexpr int kHeavyW = 8192;      // dense window width (columns)
+constexpr int kHeavyThreads = 512;
+constexpr int kLightCap = 4096;    // on-chip ESC capacity (products per unit)
+constexpr int kLightThreads = 512;
+constexpr uint64_t kLightRowMax = 1024;   // rows with at most this many products are light
+constexpr uint64_t kLightUnitMax = 3072;  // products per light unit
+
+void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
+void launch_light(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
+int heavy_blocks_per_sm();
+int light_blocks_per_sm();
+
+// ---- misc ----
+void exclusive_scan_u32_to_u64(Arena &a, const uint32_t *in, uint64_t *out, uint64_t n,
+                               cudaStream_t s);  // out has n+1 entries
+
+void digest_chunk(const uint64_t *keys, const float *vals, uint64_t n, gsparc_digest *out,
+                  cudaStream_t s);
+
+// reference-compatible index match (u64 outputs) for the stage entry point
+void index_match_compat(Arena &a, uint64_t nx, const uint64_t *xkeys, int x_ncbits, uint64_t ny,
+                        const uint64_t *ykeys, int y_nfbits, uint64_t *pos, uint64_t *cnt,
+                        uint64_t *prefix, cudaStream_t s);
+
+}  // namespace gs

@@ -1,0 +1,233 @@
+/*
+ * gsparc_b200.h -- C ABI of the B200-native sparse tensor contraction engine.
+ *
+ * Z = X x_{cx,cy} Y for two sparse COO tensors, computed the way the reference
+ * (seohyeon0322/GSPARC) computes it: linearise each operand into 64-bit keys,
+ * sort, match X and Y on their contract keys, accumulate matched products
+ * into output keys (x_free << Y_nfbits) | y_free, memory-aware chunking of the
+ * output.  Every function returns a status; none exits the process.
+ *
+ * Plain C: pointers and sizes only.  Streams are passed as `void *` holding a
+ * cudaStream_t (NULL = the legacy default stream).
+ *
+ * Reference interfaces each entry point replaces are cited per declaration as
+ * path:line inside the reference repository.
+ */
+#ifndef GSPARC_B200_H
+#define GSPARC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference exits on every error
+ * (src/common/cuda_helper.cpp:83-92, src/gsparc/cuda_memory.cpp:78,89,
+ *  include/gsparc/sptc.cuh:209-210); these are returned instead. */
+typedef enum {
+    GSPARC_OK = 0,
+    GSPARC_EINVAL = 1,       /* bad argument / malformed input            */
+    GSPARC_ENOMEM = 2,       /* HBM budget or host memory exhausted        */
+    GSPARC_ECUDA = 3,        /* CUDA runtime error                         */
+    GSPARC_EIO = 4,          /* file could not be read / written           */
+    GSPARC_ETIMEOUT = 5,     /* a bounded device wait ran out              */
+    GSPARC_EUNSUPPORTED = 6, /* valid input outside the supported envelope */
+    GSPARC_EINTERNAL = 7,    /* device-side consistency check failed       */
+    GSPARC_ECALLBACK = 8     /* an output-sink callback asked to stop      */
+} gsparc_status;
+
+typedef struct gsparc_ctx gsparc_ctx;
+typedef struct gsparc_tensor gsparc_tensor;
+
+/* SoA COO tensor (0-based indices, float values).
+ * Replaces gsparc::SparseTensor<uint64_t,float> (include/gsparc/sparse_tensor.hpp:12-44):
+ * indices[m][k] / values[k]. */
+typedef struct {
+    int order;                   /* number of modes (1..32)                   */
+    const uint64_t *dims;        /* [order] mode sizes (host memory)          */
+    uint64_t nnz;
+    const uint64_t *const *idx;  /* [order] pointers to nnz indices each      */
+    const float *val;            /* [nnz]                                     */
+    int on_device;               /* 0: idx/val are host pointers, 1: device   */
+} gsparc_coo;
+
+/* Accumulator selection, the reference's -d flag (src/gsparc/cmdline_opts.cpp:169-172,
+ * include/gsparc/sptc.cuh:201-218). */
+enum { GSPARC_ACCUM_ESC = -1, GSPARC_ACCUM_AUTO = 0, GSPARC_ACCUM_DENSE = 1 };
+
+/* Output sink kinds. */
+enum {
+    GSPARC_SINK_DISCARD = 0, /* compute every chunk in HBM, then drop it      */
+    GSPARC_SINK_DEVICE = 1,  /* call on_chunk with device pointers per chunk  */
+    GSPARC_SINK_HOST = 2     /* copy chunks into host_keys/host_vals          */
+};
+
+/* Per-chunk callback.  keys/vals hold n output nonzeros in ascending key
+ * order; first is the global index of the chunk's first nonzero.  on_device
+ * tells where keys/vals live.  Return 0 to continue, nonzero to stop
+ * (gsparc_sptc then returns GSPARC_ECALLBACK). */
+typedef int (*gsparc_chunk_fn)(void *user, const uint64_t *keys, const float *vals,
+                               uint64_t n, uint64_t first, int on_device);
+
+/* Output sink.  The reference never returns Z: it copies each ESC chunk into
+ * one reused pinned buffer and drops it (include/gsparc/contraction.cuh:554-561,596-597). */
+typedef struct {
+    int kind;
+    gsparc_chunk_fn on_chunk; /* optional for DISCARD / HOST                   */
+    void *user;
+    /* HOST sink: destination arrays.  If host_capacity >= nnz(Z) the whole Z
+     * lands there in order; otherwise every chunk overwrites the arrays from
+     * index 0 and on_chunk is called after each copy (ring mode, like the
+     * reference's reused pinned buffer).  Page-locked memory copies fastest. */
+    uint64_t *host_keys;
+    float *host_vals;
+    uint64_t host_capacity;
+    uint64_t max_chunk_nnz;   /* 0 = derive from the HBM budget                */
+} gsparc_sink;
+
+/* Statistics of one contraction (the reference prints these to stderr,
+ * main.cu:384-433). Times are milliseconds of device time per stage. */
+typedef struct {
+    uint64_t ir_nnz;          /* matched products (indexMatch.cuh:285)        */
+    uint64_t nnz;             /* output nonzeros ("Result NNZ")               */
+    uint64_t nnz_x, nnz_y;
+    uint64_t rows;            /* distinct X free indices                      */
+    uint64_t heavy_rows;      /* rows taken by the windowed dense accumulator */
+    uint64_t chunks;          /* output chunks streamed                       */
+    int nbits_x, nbits_y, ncbits, nfbits_x, nfbits_y;
+    int accumulator;          /* accumulator actually used (GSPARC_ACCUM_*)   */
+    double t_linearize_ms;    /* SLITOM construction (linearise)              */
+    double t_sort_ms;         /* SLITOM sort                                  */
+    double t_match_ms;        /* index match + row table                      */
+    double t_plan_ms;         /* symbolic pass + chunk planning               */
+    double t_contract_ms;     /* numeric accumulation                         */
+    double t_output_ms;       /* output delivery (copies, callbacks)          */
+    double t_total_ms;
+    uint64_t bytes_h2d, bytes_d2h;
+    uint64_t kernel_launches; /* this library's own kernels launched           */
+    double t_numeric_kernel_ms; /* device time of the numeric accumulation kernels */
+} gsparc_stats;
+
+/* ---- version / errors ---------------------------------------------------- */
+const char *gsparc_version(void);
+const char *gsparc_status_string(gsparc_status st);
+/* Message of the last failing call on this thread (empty if none). */
+const char *gsparc_last_error(void);
+
+/* ---- context -------------------------------------------------------------- */
+/* Replaces CudaMemoryPool(id) (src/gsparc/cuda_memory.cpp:17-30), which
+ * claimed all free HBM minus 256 MiB; the context instead admits device
+ * allocations up to hbm_budget_bytes (0 = 90% of the device's free memory). */
+gsparc_status gsparc_ctx_create(int device, uint64_t hbm_budget_bytes, gsparc_ctx **out);
+gsparc_status gsparc_ctx_destroy(gsparc_ctx *ctx);
+/* Bytes currently allocated by the context and its high-water mark. */
+gsparc_status gsparc_ctx_memory(gsparc_ctx *ctx, uint64_t *in_use, uint64_t *peak,
+                                uint64_t *budget);
+
+/* ---- resident operands ---------------------------------------------------- */
+/* Copy (or adopt, when on_device) a COO tensor into the context.  Replaces the
+ * H2D copies of SortSlitomXY / SpTC (include/gsparc/sort.cuh:79-107,
+ * include/gsparc/sptc.cuh:86-91,128-134).  The tensor stays resident until
+ * gsparc_tensor_free. */
+gsparc_status gsparc_tensor_upload(gsparc_ctx *ctx, const gsparc_coo *coo, void *stream,
+                                   gsparc_tensor **out);
+gsparc_status gsparc_tensor_free(gsparc_ctx *ctx, gsparc_tensor *t);
+gsparc_status gsparc_tensor_info(const gsparc_tensor *t, int *order, uint64_t *dims /*[32]*/,
+                                 uint64_t *nnz);
+
+/* ---- the contraction ------------------------------------------------------ */
+/* Z = X x_{cx,cy} Y.  Replaces gsparc::SpTC (include/gsparc/sptc.cuh:16-360)
+ * together with the TensorManager steps main.cu:293-321 runs before it
+ * (ConvertTensor, SortSlitomXY, Partition).  cx[i] of X is contracted with
+ * cy[i] of Y.  accum is GSPARC_ACCUM_*.  Work is ordered on `stream`;
+ * the call returns after the last chunk was delivered. */
+gsparc_status gsparc_sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y,
+                          int ncmodes, const int *cx, const int *cy, int accum,
+                          const gsparc_sink *sink, gsparc_stats *stats, void *stream);
+
+/* Row-sharded form for multi-GPU runs: only the X free indices (output rows)
+ * of shard `shard` of `nshards` are contracted.  Shards split the rows at
+ * equal matched-product mass; the union of all shards is Z, and shard s's
+ * output keys all precede shard s+1's.  Replaces the round-robin X partition
+ * over GPUs of include/gsparc/sptc.cuh:42-45. */
+gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y,
+                                int ncmodes, const int *cx, const int *cy, int accum,
+                                int shard, int nshards,
+                                const gsparc_sink *sink, gsparc_stats *stats, void *stream);
+
+/* ---- host helpers (no GPU needed) ---------------------------------------- */
+/* Parse a .tns file: 1-based text COO, one nonzero per line, order = tokens of
+ * the first line minus one, dims[m] = largest index + 1.  Replaces
+ * IOManager::ParseFromFile / parse_metadata_and_data
+ * (include/gsparc/io_manager.tpp:24-34,75-259).  Arrays are malloc'd by the
+ * library (free with gsparc_free_host); idx is SoA: idx[m*nnz + k]. */
+gsparc_status gsparc_read_tns(const char *path, int nthreads, int *order, uint64_t *dims /*[32]*/,
+                              uint64_t *nnz, uint64_t **idx, float **val);
+/* Write 1-based text COO with %.9g values. */
+gsparc_status gsparc_write_tns(const char *path, int order, uint64_t nnz,
+                               const uint64_t *idx /* SoA idx[m*nnz+k] */, const float *val);
+void gsparc_free_host(void *p);
+
+/* Bit layout of one operand.  Replaces TensorManager::compute_nbtis,
+ * setup_slitom and create_mask (include/gsparc/tensor_manager.tpp:91-210):
+ * bits[m] = 64 - clz(dims[m]-1) (0 for size-1 modes), free modes in
+ * ascending order, the first free (contract) mode in the highest bits.
+ * shift[m] is the position of mode m inside its part. */
+gsparc_status gsparc_layout(int order, const uint64_t *dims, int ncmodes, const int *cmodes,
+                            int *bits, int *shift, int *is_contract,
+                            int *ncbits, int *nfbits);
+
+/* Split rows into nshards ranges of near-equal product mass: row_prod[r] is
+ * the matched products of row r; bounds gets nshards+1 row indices. */
+gsparc_status gsparc_plan_shards(const uint64_t *row_prod, uint64_t nrows, int nshards,
+                                 uint64_t *bounds);
+
+/* ---- stage entry points (device pointers, for parity tests) -------------- */
+/* Linearise one operand into 64-bit keys.  role 0 = X layout
+ * (free << ncbits | contract), role 1 = Y layout (contract << nfbits | free).
+ * Replaces TensorManager::ConvertTensor (include/gsparc/tensor_manager.tpp:213-298),
+ * whose host pdep loop becomes a device kernel.  d_idx is SoA on the device:
+ * d_idx[m*nnz + k]. */
+gsparc_status gsparc_linearize(int order, const uint64_t *dims, int ncmodes, const int *cmodes,
+                               int role, uint64_t nnz, const uint64_t *d_idx,
+                               uint64_t *d_keys, void *stream);
+
+/* Stable sort of (key, value) pairs by the low `nbits` bits of the key.
+ * Replaces sort_64 (include/gsparc/sort.cuh:40-159).  In place. */
+gsparc_status gsparc_sort_pairs(gsparc_ctx *ctx, uint64_t n, uint64_t *d_keys, float *d_vals,
+                                int nbits, void *stream);
+
+/* For sorted X keys and sorted Y keys: pos[i] = first Y index whose contract
+ * key equals X[i]'s, cnt[i] = length of that run (0 and 0 if none),
+ * prefix[0] = 0, prefix[i+1] = prefix[i] + cnt[i]; *ir = prefix[nx].
+ * Replaces IndexMatch / compute_result_size_cuda
+ * (include/gsparc/indexMatch.cuh:67-118,231-287). */
+gsparc_status gsparc_index_match(gsparc_ctx *ctx, uint64_t nx, const uint64_t *d_xkeys,
+                                 int x_ncbits, uint64_t ny, const uint64_t *d_ykeys,
+                                 int y_nfbits, uint64_t *d_pos, uint64_t *d_cnt,
+                                 uint64_t *d_prefix, uint64_t *ir, void *stream);
+
+/* ---- verification digest of an output chunk ------------------------------ */
+/* Order-independent digest of n output nonzeros on the device: count, a sum
+ * of mixed keys, how many neighbours are not strictly increasing, the first
+ * and last key, and the values summed in double precision.  Used to verify
+ * outputs too large to bring to the host.  No counterpart in the reference
+ * (which never inspects its output). */
+typedef struct {
+    uint64_t n;
+    uint64_t key_hash;      /* sum over keys of splitmix64(key), mod 2^64      */
+    uint64_t unsorted;      /* #i with keys[i] >= keys[i+1]                    */
+    uint64_t first_key, last_key;
+    double val_sum;         /* sum of values (double)                         */
+    double val_abs_sum;     /* sum of |values| (double)                       */
+} gsparc_digest;
+gsparc_status gsparc_digest_chunk(const uint64_t *d_keys, const float *d_vals, uint64_t n,
+                                  gsparc_digest *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSPARC_B200_H */

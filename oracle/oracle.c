@@ -1,0 +1,510 @@
+/*
+ * oracle.c -- CPU restatement of GSPARC's SpTC path.  TEST INFRASTRUCTURE ONLY.
+ *
+ * This file is the checker for the CUDA engine in gsparc_b200/: only the tests,
+ * the smoke check and the CPU-baseline leg of the benchmark load it.  The
+ * product path never calls it.
+ *
+ * It restates, in plain C, the semantics of the reference's path
+ * (seohyeon0322/GSPARC), step by step:
+ *
+ *   parse .tns          include/gsparc/io_manager.tpp:75-259 (dims = max idx + 1, :213,:250-256)
+ *   mode bit widths     include/gsparc/tensor_manager.tpp:107-125 (64 - clz(dim-1))
+ *   free-mode order     include/gsparc/tensor_manager.tpp:64-88
+ *   masks / shifts      include/gsparc/tensor_manager.tpp:153-174 (first mode highest)
+ *   linearise           include/gsparc/tensor_manager.tpp:246-268 (X: f<<ncbits|c)
+ *                       include/gsparc/tensor_manager.tpp:270-294 (Y: c<<nfbits|f)
+ *   stable sort by key  include/gsparc/sort.cuh:90-108 (CUB radix sort, stable)
+ *   index match         include/gsparc/indexMatch.cuh:20-44,67-118,231-287
+ *   ESC expand          include/gsparc/contraction.cuh:100-141 (key x_f<<Y_nfbits | y_f)
+ *   sort + reduce       include/gsparc/contraction.cuh:506-537 (ascending keys, Sum)
+ *
+ * nnz follows the ESC semantics: every distinct output key that received at
+ * least one product counts, including sums that cancel to exactly zero.
+ * Values are summed in double precision.  Mode widths of one bit-width 0 are
+ * used for size-1 modes (the reference's clz(0) is undefined there).
+ *
+ * Parity status: the restatement is pinned against outputs of the
+ * reference's own CPU SpTC (baselines/Sparta, built from source by
+ * oracle/Makefile) through fixtures in tests/golden/.
+ */
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+
+#define OR_OK 0
+#define OR_EINVAL 1
+#define OR_ENOMEM 2
+#define OR_EIO 4
+
+/* ------------------------------------------------------------------ bits */
+
+/* tensor_manager.tpp:109 -- bits = 64 - clz(dim - 1); dim 1 gives 0 here. */
+int oracle_mode_bits(uint64_t dim)
+{
+    if (dim <= 1)
+        return 0;
+    return 64 - __builtin_clzll(dim - 1);
+}
+
+/*
+ * Layout of one operand: shift[m] for every mode m (position of the mode's
+ * field inside its free or contract part), ncbits, nfbits.
+ * Free modes are the non-contract modes in ascending order (tensor_manager.tpp:64-88);
+ * the LAST free (contract) mode sits in the lowest bits and the first one in
+ * the highest bits (tensor_manager.tpp:153-174).
+ */
+int oracle_layout(int order, const uint64_t *dims, int nc, const int *cpos,
+                  int *shift, int *is_contract, int *fpos_out,
+                  int *ncbits, int *nfbits)
+{
+    int fpos[64];
+    int nf = 0;
+    if (order <= 0 || order > 64 || nc < 0 || nc > order)
+        return OR_EINVAL;
+    for (int m = 0; m < order; ++m)
+        is_contract[m] = 0;
+    for (int i = 0; i < nc; ++i) {
+        if (cpos[i] < 0 || cpos[i] >= order || is_contract[cpos[i]])
+            return OR_EINVAL;
+        is_contract[cpos[i]] = 1;
+    }
+    for (int m = 0; m < order; ++m)
+        if (!is_contract[m])
+            fpos[nf++] = m;
+    int s = 0;
+    for (int n = nf - 1; n >= 0; --n) {
+        shift[fpos[n]] = s;
+        s += oracle_mode_bits(dims[fpos[n]]);
+    }
+    *nfbits = s;
+    s = 0;
+    for (int n = nc - 1; n >= 0; --n) {
+        shift[cpos[n]] = s;
+        s += oracle_mode_bits(dims[cpos[n]]);
+    }
+    *ncbits = s;
+    if (fpos_out)
+        for (int i = 0; i < nf; ++i)
+            fpos_out[i] = fpos[i];
+    return OR_OK;
+}
+
+/*
+ * Linearise one operand.  role 0 = X layout (f << ncbits | c),
+ * role 1 = Y layout (c << nfbits | f).  idx is SoA: idx[m*nnz + k].
+ */
+int oracle_linearize(int order, const uint64_t *dims, int nc, const int *cpos,
+                     int role, uint64_t nnz, const uint64_t *idx, uint64_t *keys)
+{
+    int shift[64], isc[64], ncb, nfb;
+    int st = oracle_layout(order, dims, nc, cpos, shift, isc, NULL, &ncb, &nfb);
+    if (st)
+        return st;
+    if (ncb + nfb > 64)
+        return OR_EINVAL;
+    for (uint64_t k = 0; k < nnz; ++k) {
+        uint64_t f = 0, c = 0;
+        for (int m = 0; m < order; ++m) {
+            uint64_t v = idx[(uint64_t)m * nnz + k];
+            if (isc[m])
+                c |= v << shift[m];
+            else
+                f |= v << shift[m];
+        }
+        keys[k] = role == 0 ? ((ncb >= 64 ? 0 : (f << ncb)) | c)
+                            : ((nfb >= 64 ? 0 : (c << nfb)) | f);
+    }
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------- sorting */
+
+/* Stable LSD radix sort of keys with a permutation payload (16-bit digits). */
+static int stable_sort_perm(uint64_t n, const uint64_t *keys, int nbits, uint64_t *perm)
+{
+    uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * (n ? n : 1));
+    uint64_t *cnt = (uint64_t *)malloc(sizeof(uint64_t) * 65536);
+    if (!tmp || !cnt) {
+        free(tmp);
+        free(cnt);
+        return OR_ENOMEM;
+    }
+    for (uint64_t i = 0; i < n; ++i)
+        perm[i] = i;
+    uint64_t *a = perm, *b = tmp;
+    for (int sh = 0; sh < nbits; sh += 16) {
+        memset(cnt, 0, sizeof(uint64_t) * 65536);
+        for (uint64_t i = 0; i < n; ++i)
+            cnt[(keys[a[i]] >> sh) & 0xFFFF]++;
+        uint64_t run = 0;
+        for (int d = 0; d < 65536; ++d) {
+            uint64_t c = cnt[d];
+            cnt[d] = run;
+            run += c;
+        }
+        for (uint64_t i = 0; i < n; ++i)
+            b[cnt[(keys[a[i]] >> sh) & 0xFFFF]++] = a[i];
+        uint64_t *t = a;
+        a = b;
+        b = t;
+    }
+    if (a != perm)
+        memcpy(perm, a, sizeof(uint64_t) * n);
+    free(tmp);
+    free(cnt);
+    return OR_OK;
+}
+
+/* Sort (keys, vals) in place by key, stable (sort.cuh:90-108 semantics). */
+int oracle_sort_pairs(uint64_t n, uint64_t *keys, float *vals, int nbits)
+{
+    uint64_t *perm = (uint64_t *)malloc(sizeof(uint64_t) * (n ? n : 1));
+    uint64_t *k2 = (uint64_t *)malloc(sizeof(uint64_t) * (n ? n : 1));
+    float *v2 = (float *)malloc(sizeof(float) * (n ? n : 1));
+    if (!perm || !k2 || !v2) {
+        free(perm);
+        free(k2);
+        free(v2);
+        return OR_ENOMEM;
+    }
+    int st = stable_sort_perm(n, keys, nbits, perm);
+    if (!st) {
+        for (uint64_t i = 0; i < n; ++i) {
+            k2[i] = keys[perm[i]];
+            v2[i] = vals[perm[i]];
+        }
+        memcpy(keys, k2, sizeof(uint64_t) * n);
+        memcpy(vals, v2, sizeof(float) * n);
+    }
+    free(perm);
+    free(k2);
+    free(v2);
+    return st;
+}
+
+/* ------------------------------------------------------------ matching */
+
+/*
+ * indexMatch.cuh:20-44 + :67-118 -- for every X nonzero (sorted X keys), the
+ * first Y position whose contract key (y >> fbits) equals x & cmask, and the
+ * length of that run.  pos is left 0 and cnt 0 when there is no match
+ * (the reference memsets both arrays, sptc.cuh:144-146).
+ * prefix[0] = 0, prefix[i+1] = cnt[0] + ... + cnt[i] (indexMatch.cuh:275-285).
+ */
+int oracle_index_match(uint64_t nx, const uint64_t *xkeys, int x_ncbits,
+                       uint64_t ny, const uint64_t *ykeys, int y_nfbits,
+                       uint64_t *pos, uint64_t *cnt, uint64_t *prefix)
+{
+    uint64_t cmask = x_ncbits >= 64 ? ~0ull : ((1ull << x_ncbits) - 1);
+    prefix[0] = 0;
+    for (uint64_t i = 0; i < nx; ++i) {
+        uint64_t c = xkeys[i] & cmask;
+        uint64_t lo = 0, hi = ny;
+        while (lo < hi) {
+            uint64_t mid = lo + (hi - lo) / 2;
+            uint64_t yc = y_nfbits >= 64 ? 0 : (ykeys[mid] >> y_nfbits);
+            if (yc < c)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        uint64_t n = 0;
+        if (lo < ny && (y_nfbits >= 64 ? 0 : (ykeys[lo] >> y_nfbits)) == c) {
+            pos[i] = lo;
+            while (lo + n < ny && (y_nfbits >= 64 ? 0 : (ykeys[lo + n] >> y_nfbits)) == c)
+                ++n;
+        } else {
+            pos[i] = 0;
+        }
+        cnt[i] = n;
+        prefix[i + 1] = prefix[i] + n;
+    }
+    return OR_OK;
+}
+
+/* --------------------------------------------------------------- SpTC */
+
+typedef struct {
+    uint64_t ir_nnz;     /* matched products */
+    uint64_t nnz;        /* distinct output keys */
+    int x_nfbits, y_nfbits, ncbits_x, ncbits_y;
+    uint64_t *keys;      /* [nnz] ascending output keys (x_f << y_nfbits | y_f) */
+    double *vals;        /* [nnz] FP64 sums */
+    double *abs_sums;    /* [nnz] sum of |products| (scale for tolerances) */
+    uint64_t *nprod;     /* [nnz] products per key */
+} oracle_result;
+
+void oracle_free(oracle_result *r)
+{
+    if (!r)
+        return;
+    free(r->keys);
+    free(r->vals);
+    free(r->abs_sums);
+    free(r->nprod);
+    free(r);
+}
+
+/*
+ * Full path: linearise X and Y, stable-sort both, match, expand every product
+ * with key (x_f << Y_nfbits) | y_f (contraction.cuh:132-137), sort the products
+ * by key and reduce equal keys.  idx arrays are SoA, 0-based.
+ * max_products bounds the expansion (the oracle is for small cases).
+ */
+int oracle_sptc(int ox, const uint64_t *dx, uint64_t nx, const uint64_t *ix, const float *vx,
+                int oy, const uint64_t *dy, uint64_t ny, const uint64_t *iy, const float *vy,
+                int nc, const int *cx, const int *cy, uint64_t max_products,
+                oracle_result **out)
+{
+    int shx[64], iscx[64], ncx, nfx, shy[64], iscy[64], ncy, nfy;
+    int st;
+    *out = NULL;
+    if ((st = oracle_layout(ox, dx, nc, cx, shx, iscx, NULL, &ncx, &nfx)))
+        return st;
+    if ((st = oracle_layout(oy, dy, nc, cy, shy, iscy, NULL, &ncy, &nfy)))
+        return st;
+    for (int i = 0; i < nc; ++i)
+        if (oracle_mode_bits(dx[cx[i]]) != oracle_mode_bits(dy[cy[i]]))
+            return OR_EINVAL;
+    if (ncx + nfx > 64 || ncy + nfy > 64 || nfx + nfy > 64)
+        return OR_EINVAL;
+
+    oracle_result *r = (oracle_result *)calloc(1, sizeof(oracle_result));
+    uint64_t *kx = (uint64_t *)malloc(8 * (nx ? nx : 1));
+    uint64_t *ky = (uint64_t *)malloc(8 * (ny ? ny : 1));
+    float *sx = (float *)malloc(4 * (nx ? nx : 1));
+    float *sy = (float *)malloc(4 * (ny ? ny : 1));
+    uint64_t *pos = (uint64_t *)malloc(8 * (nx ? nx : 1));
+    uint64_t *cnt = (uint64_t *)malloc(8 * (nx ? nx : 1));
+    uint64_t *pre = (uint64_t *)malloc(8 * (nx + 1));
+    if (!r || !kx || !ky || !sx || !sy || !pos || !cnt || !pre) {
+        st = OR_ENOMEM;
+        goto fail;
+    }
+    r->x_nfbits = nfx;
+    r->y_nfbits = nfy;
+    r->ncbits_x = ncx;
+    r->ncbits_y = ncy;
+    oracle_linearize(ox, dx, nc, cx, 0, nx, ix, kx);
+    oracle_linearize(oy, dy, nc, cy, 1, ny, iy, ky);
+    memcpy(sx, vx, 4 * nx);
+    memcpy(sy, vy, 4 * ny);
+    if ((st = oracle_sort_pairs(nx, kx, sx, ncx + nfx)))
+        goto fail;
+    if ((st = oracle_sort_pairs(ny, ky, sy, ncy + nfy)))
+        goto fail;
+    oracle_index_match(nx, kx, ncx, ny, ky, nfy, pos, cnt, pre);
+    uint64_t ir = pre[nx];
+    r->ir_nnz = ir;
+    if (ir > max_products) {
+        st = OR_ENOMEM;
+        goto fail;
+    }
+    {
+        uint64_t *pk = (uint64_t *)malloc(8 * (ir ? ir : 1));
+        double *pv = (double *)malloc(8 * (ir ? ir : 1));
+        uint64_t *perm = (uint64_t *)malloc(8 * (ir ? ir : 1));
+        if (!pk || !pv || !perm) {
+            free(pk);
+            free(pv);
+            free(perm);
+            st = OR_ENOMEM;
+            goto fail;
+        }
+        uint64_t fmask = nfy >= 64 ? ~0ull : ((1ull << nfy) - 1);
+        uint64_t p = 0;
+        for (uint64_t i = 0; i < nx; ++i) {
+            uint64_t xf = ncx >= 64 ? 0 : (kx[i] >> ncx);
+            for (uint64_t j = 0; j < cnt[i]; ++j) {
+                uint64_t yk = ky[pos[i] + j];
+                pk[p] = (nfy >= 64 ? 0 : (xf << nfy)) | (yk & fmask);
+                pv[p] = (double)sx[i] * (double)sy[pos[i] + j];
+                ++p;
+            }
+        }
+        st = stable_sort_perm(ir, pk, nfx + nfy, perm);
+        if (st) {
+            free(pk);
+            free(pv);
+            free(perm);
+            goto fail;
+        }
+        uint64_t nz = 0;
+        for (uint64_t q = 0; q < ir; ++q)
+            if (q == 0 || pk[perm[q]] != pk[perm[q - 1]])
+                ++nz;
+        r->nnz = nz;
+        r->keys = (uint64_t *)malloc(8 * (nz ? nz : 1));
+        r->vals = (double *)malloc(8 * (nz ? nz : 1));
+        r->abs_sums = (double *)malloc(8 * (nz ? nz : 1));
+        r->nprod = (uint64_t *)malloc(8 * (nz ? nz : 1));
+        if (!r->keys || !r->vals || !r->abs_sums || !r->nprod) {
+            free(pk);
+            free(pv);
+            free(perm);
+            st = OR_ENOMEM;
+            goto fail;
+        }
+        int64_t o = -1;
+        for (uint64_t q = 0; q < ir; ++q) {
+            uint64_t k = pk[perm[q]];
+            double v = pv[perm[q]];
+            if (q == 0 || k != pk[perm[q - 1]]) {
+                ++o;
+                r->keys[o] = k;
+                r->vals[o] = 0.0;
+                r->abs_sums[o] = 0.0;
+                r->nprod[o] = 0;
+            }
+            r->vals[o] += v;
+            r->abs_sums[o] += fabs(v);
+            r->nprod[o] += 1;
+        }
+        free(pk);
+        free(pv);
+        free(perm);
+    }
+    free(kx);
+    free(ky);
+    free(sx);
+    free(sy);
+    free(pos);
+    free(cnt);
+    free(pre);
+    *out = r;
+    return OR_OK;
+fail:
+    free(kx);
+    free(ky);
+    free(sx);
+    free(sy);
+    free(pos);
+    free(cnt);
+    free(pre);
+    oracle_free(r);
+    return st;
+}
+
+/* ---------------------------------------------------------- .tns input */
+
+/*
+ * io_manager.tpp:75-259: order = (#tokens of the first line) - 1; every line
+ * holding tokens is one nonzero; indices are 1-based and stored 0-based;
+ * dims[m] = max index + 1; values are parsed as double and cast to float.
+ * Returns nnz and order via the out parameters; idx (SoA) and vals are
+ * malloc'd and owned by the caller (free with oracle_free_buf).
+ */
+int oracle_read_tns(const char *path, int *order_out, uint64_t *nnz_out,
+                    uint64_t *dims_out /* [64] */, uint64_t **idx_out, float **val_out)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f)
+        return OR_EIO;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    rewind(f);
+    char *buf = (char *)malloc((size_t)sz + 1);
+    if (!buf) {
+        fclose(f);
+        return OR_ENOMEM;
+    }
+    if (fread(buf, 1, (size_t)sz, f) != (size_t)sz) {
+        fclose(f);
+        free(buf);
+        return OR_EIO;
+    }
+    fclose(f);
+    buf[sz] = '\0';
+    /* order from the first line */
+    int ntok = 0;
+    {
+        char *p = buf;
+        while (*p && *p != '\n') {
+            while (*p == ' ' || *p == '\t' || *p == '\r')
+                ++p;
+            if (!*p || *p == '\n')
+                break;
+            ++ntok;
+            while (*p && *p != ' ' && *p != '\t' && *p != '\n' && *p != '\r')
+                ++p;
+        }
+    }
+    int order = ntok - 1;
+    if (order <= 0 || order > 64) {
+        free(buf);
+        return OR_EINVAL;
+    }
+    uint64_t lines = 0;
+    for (long i = 0; i < sz; ++i)
+        if (buf[i] == '\n')
+            ++lines;
+    if (sz > 0 && buf[sz - 1] != '\n')
+        ++lines;
+    uint64_t *idx = (uint64_t *)malloc(8 * (size_t)order * (lines ? lines : 1));
+    float *val = (float *)malloc(4 * (lines ? lines : 1));
+    if (!idx || !val) {
+        free(buf);
+        free(idx);
+        free(val);
+        return OR_ENOMEM;
+    }
+    uint64_t *tmp = (uint64_t *)malloc(8 * (size_t)order * (lines ? lines : 1));
+    float *tv = (float *)malloc(4 * (lines ? lines : 1));
+    for (int m = 0; m < order; ++m)
+        dims_out[m] = 0;
+    uint64_t n = 0;
+    char *p = buf;
+    while (*p) {
+        char *line = p;
+        char *e = strchr(p, '\n');
+        if (e) {
+            *e = '\0';
+            p = e + 1;
+        } else {
+            p = line + strlen(line);
+        }
+        char *s = line;
+        while (*s == ' ' || *s == '\t' || *s == '\r')
+            ++s;
+        if (!*s)
+            continue;
+        int m = 0;
+        char *q = s;
+        for (; m < order; ++m) {
+            char *endp;
+            unsigned long long v = strtoull(q, &endp, 10);
+            if (endp == q || v == 0) {
+                free(buf); free(idx); free(val); free(tmp); free(tv);
+                return OR_EINVAL;
+            }
+            tmp[(size_t)m * lines + n] = (uint64_t)(v - 1);
+            if (v > dims_out[m])
+                dims_out[m] = v;
+            q = endp;
+        }
+        char *endp;
+        double d = strtod(q, &endp);
+        if (endp == q) {
+            free(buf); free(idx); free(val); free(tmp); free(tv);
+            return OR_EINVAL;
+        }
+        tv[n] = (float)d;
+        ++n;
+    }
+    for (int m = 0; m < order; ++m)
+        memcpy(idx + (size_t)m * n, tmp + (size_t)m * lines, 8 * n);
+    memcpy(val, tv, 4 * n);
+    free(tmp);
+    free(tv);
+    free(buf);
+    *order_out = order;
+    *nnz_out = n;
+    *idx_out = idx;
+    *val_out = val;
+    return OR_OK;
+}
+
+void oracle_free_buf(void *p) { free(p); }

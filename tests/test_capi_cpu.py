@@ -1,0 +1,137 @@
+"""Host-side checks of the C ABI library that need no GPU: it loads, exports
+every declared entry point, and its host helpers (bit layout, .tns I/O, shard
+planning, CLI argument handling) agree with the oracle / reference rules."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import gsparc_b200 as gb
+import oracle_bind as ob
+from gsparc_b200 import synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "gsparc_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gsparc_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = gb.lib()
+    decl = _declared()
+    assert len(decl) >= 20
+    for name in decl:
+        assert hasattr(L, name), name
+    assert set(gb.EXPORTS) <= set(decl)
+
+
+def test_version_and_status_strings():
+    assert "sm_100a" in gb.version()
+    assert gb.lib().gsparc_status_string(2) == b"out of memory"
+
+
+@pytest.mark.parametrize("dims,cm", [([2482, 2862, 14036, 17], [2, 3]), ([13, 40, 17], [2, 1]),
+                                     ([1000, 1000, 1000], [2]), ([7, 1, 9, 2], [3, 0]),
+                                     ([2**40, 2**20, 3], [1])])
+def test_layout_matches_oracle(dims, cm):
+    bits, shift, isc, ncb, nfb = gb.layout(dims, cm)
+    oshift, oisc, oncb, onfb = ob.layout(dims, cm)
+    assert (ncb, nfb) == (oncb, onfb)
+    assert list(shift) == list(oshift) and list(isc) == list(oisc)
+    assert list(bits) == [ob.mode_bits(d) for d in dims]
+
+
+def test_layout_rejects_bad_modes():
+    with pytest.raises(gb.GsparcError):
+        gb.layout([10, 10], [2])
+    with pytest.raises(gb.GsparcError):
+        gb.layout([10, 10, 10], [1, 1])
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_read_tns_matches_oracle_parser(tmp_path, seed):
+    t = synth.make_tensor([50, 7, 300], 3000, ["uniform", ("zipf", 1.3), "uniform"], "normal", seed)
+    p = str(tmp_path / "a.tns")
+    synth.write_tns(p, t)
+    a = gb.read_tns(p, nthreads=4)
+    b = ob.read_tns(p)
+    assert a.dims == b.dims == t.dims
+    assert np.array_equal(a.idx, b.idx) and np.array_equal(a.idx, t.idx)
+    assert np.array_equal(a.val, b.val) and np.array_equal(a.val, t.val)
+
+
+def test_read_tns_tolerates_blank_lines_tabs_crlf(tmp_path):
+    p = tmp_path / "b.tns"
+    p.write_bytes(b"1\t2 3 0.5\r\n\n  4 5 6\t-1.25e-3\r\n2 2 2 7\n\n")
+    a = gb.read_tns(str(p), nthreads=3)
+    assert a.dims == [4, 5, 6]
+    assert a.idx.tolist() == [[0, 3, 1], [1, 4, 1], [2, 5, 1]]
+    assert np.allclose(a.val, [0.5, -1.25e-3, 7.0])
+
+
+@pytest.mark.parametrize("content", [b"1 2 3\n0 1 1 2.0\n", b"1 2 3 1.0\n1 2\n", b"",
+                                     b"1 x 3 1.0\n"])
+def test_read_tns_reports_malformed_input(tmp_path, content):
+    p = tmp_path / "bad.tns"
+    p.write_bytes(content)
+    with pytest.raises(gb.GsparcError) as e:
+        gb.read_tns(str(p))
+    assert e.value.status == 1
+
+
+def test_read_tns_missing_file():
+    with pytest.raises(gb.GsparcError) as e:
+        gb.read_tns("/nonexistent/x.tns")
+    assert e.value.status == 4
+
+
+def test_write_tns_round_trip(tmp_path):
+    t = synth.make_tensor([9, 99, 999], 500, ["uniform"] * 3, "u11", 5)
+    p = str(tmp_path / "w.tns")
+    gb.write_tns(p, t.idx, t.val)
+    a = gb.read_tns(p)
+    assert np.array_equal(a.idx, t.idx) and np.array_equal(a.val, t.val)
+
+
+def test_plan_shards_balances_product_mass():
+    rng = np.random.default_rng(0)
+    rp = (rng.pareto(1.2, 100000) * 100).astype(np.uint64)
+    for n in (1, 2, 4, 8):
+        b = gb.plan_shards(rp, n)
+        assert b[0] == 0 and b[-1] == rp.shape[0] and np.all(np.diff(b.astype(np.int64)) >= 0)
+        mass = [int(rp[b[i]:b[i + 1]].sum()) for i in range(n)]
+        assert sum(mass) == int(rp.sum())
+        assert max(mass) <= int(rp.sum()) / n + int(rp.max())
+    assert list(gb.plan_shards(np.zeros(0, np.uint64), 3)) == [0, 0, 0, 0]
+
+
+def test_context_without_gpu_returns_status_not_crash():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(gb.GsparcError) as e:
+        gb.Context(0)
+    assert e.value.status in (1, 3)
+
+
+def test_cli_rejects_unsupported_and_bad_arguments(tmp_path):
+    cli = gb.CLI_PATH
+    assert os.path.exists(cli)
+    r = subprocess.run([cli, "-X", "a", "-Y", "b", "-c", "1", "-x", "0", "-y", "0", "-q"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "quantum" in r.stderr
+    r = subprocess.run([cli, "-X", "a"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+    r = subprocess.run([cli, "-X", "/none/a.tns", "-Y", "/none/b.tns", "-c", "2", "-x", "0", "1",
+                        "-y", "1", "0", "-d", "-1"], capture_output=True, text=True)
+    assert r.returncode == 1
+    # the reference's parse-time report lines (src/gsparc/cmdline_opts.cpp:92-171)
+    assert "tensor X: /none/a.tns" in r.stderr and "tensor Y: /none/b.tns" in r.stderr
+    assert "# contract modes of X: 2, contract modes: 0 1 \n" in r.stderr
+    assert "# contract modes of Y: 2, contract modes: 1 0 \n" in r.stderr
+    assert "dense_accumulator: -1" in r.stderr
