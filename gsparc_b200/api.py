@@ -332,7 +332,7 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
             parts = []
 
             def _cbh(user, k, v, n, first, on_dev):
-                if k == s.host_keys + 8 * first:
+                if first and k == s.host_keys + 8 * first:
                     return 0  # whole-Z mode: the chunk already sits at its final place
                 kk = np.ctypeslib.as_array(ctypes.cast(k, ctypes.POINTER(ctypes.c_uint64)), shape=(n,)).copy() if n else np.zeros(0, np.uint64)
                 vv = np.ctypeslib.as_array(ctypes.cast(v, ctypes.POINTER(ctypes.c_float)), shape=(n,)).copy() if n else np.zeros(0, np.float32)
@@ -364,7 +364,7 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
                                    ctypes.byref(st), ctypes.c_void_p(stream)), "sptc")
     if sink == "host":
         parts.sort(key=lambda p: p[0])
-        if parts and st.nnz <= s.host_capacity:
+        if st.nnz <= s.host_capacity:
             # whole Z fits the staging arrays: chunks landed in order
             keys = np.array(np.ctypeslib.as_array(ctypes.cast(s.host_keys, ctypes.POINTER(ctypes.c_uint64)), shape=(s.host_capacity,))[: st.nnz])
             vals = np.array(np.ctypeslib.as_array(ctypes.cast(s.host_vals, ctypes.POINTER(ctypes.c_float)), shape=(s.host_capacity,))[: st.nnz])

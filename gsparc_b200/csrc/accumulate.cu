@@ -181,8 +181,12 @@ __global__ void __launch_bounds__(kHeavyThreads) k_heavy(AccArgs a) {
                     ww &= ww - 1;
                     const uint32_t cell = (uint32_t)tid * 32 + b;
                     const float v = hi[cell] + lo[cell];
-                    a.out_keys[o] = xf_hi | a.cols[B + cell];
-                    a.out_vals[o] = v;
+                    if (o < a.out_cap) {
+                        a.out_keys[o] = xf_hi | a.cols[B + cell];
+                        a.out_vals[o] = v;
+                    } else {
+                        atomicOr(a.err, 4u);
+                    }
                     hi[cell] = -0.0f;
                     lo[cell] = 0.0f;
                     ++o;
@@ -340,8 +344,12 @@ __global__ void __launch_bounds__(kLightThreads) k_light(AccArgs a) {
                 ++e;
             } while (e < P && key[e] == k);
             const uint64_t o = a.row_off[row] - a.chunk_base + rank_in_row;
-            a.out_keys[o] = shl(a.row_xf[row], a.y_nfbits) | a.cols[(uint32_t)k];
-            a.out_vals[o] = s + c;
+            if (o < a.out_cap) {
+                a.out_keys[o] = shl(a.row_xf[row], a.y_nfbits) | a.cols[(uint32_t)k];
+                a.out_vals[o] = s + c;
+            } else {
+                atomicOr(a.err, 4u);
+            }
         }
         __syncthreads();
     }

@@ -287,6 +287,7 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
         b.chunk_base = h_off[ra] + c.first;
         b.out_keys = out_k;
         b.out_vals = out_v;
+        b.out_cap = c.n;
         b.units = dl;
         b.nunits = (uint32_t)(hl.size() / 2);
         GS_CUDA(cudaMemsetAsync(ctx->d_flag + 1, 0, 4, s));
@@ -338,6 +339,7 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
     d2h(&herr, ctx->d_flag, 1, s);
     GS_CUDA(cudaStreamSynchronize(s));
     GS_REQUIRE(!(herr & 2u), GSPARC_EINTERNAL, "light unit over capacity");
+    GS_REQUIRE(!(herr & 4u), GSPARC_EINTERNAL, "numeric pass wrote past its chunk (symbolic count mismatch)");
 
     st.t_linearize_ms = tl.ms(0, 1);
     st.t_sort_ms = tl.ms(1, 2);

@@ -82,6 +82,7 @@ struct AccArgs {
     // numeric output
     const uint64_t *row_off;   // [nrows] exclusive prefix of row_nnz
     uint64_t chunk_base;
+    uint64_t out_cap;          // capacity of out_keys/out_vals (writes beyond are skipped, err bit 4)
     uint64_t *out_keys;
     float *out_vals;
     unsigned int *err;

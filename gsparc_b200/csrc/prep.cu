@@ -134,6 +134,7 @@ __global__ void k_rows(const uint64_t *__restrict__ xkeys, int ncb, const uint32
         }
         uint32_t a = rs[r];
         uint32_t b = (r + 1 < nrows) ? rs[r + 1] : (uint32_t)nx;
+        row_start_out[r] = a;
         row_xf[r] = shr(xkeys[a], ncb);
         row_prod[r] = xprefix[b] - xprefix[a];
     }

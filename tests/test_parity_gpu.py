@@ -144,7 +144,8 @@ def test_edge_cases(ctx):
     # size-1 modes (0 bits) on both sides
     X = synth.make_tensor([30, 2, 20], 200, ["uniform"] * 3, "u11", 3)
     X = CooTensor([30, 1, 20], np.stack([X.idx[0], np.zeros_like(X.idx[1]), X.idx[2]]), X.val)
-    Y = synth.make_tensor([20, 1, 7], 100, ["uniform", "uniform", "uniform"], "u11", 4)
+    Y = synth.make_tensor([20, 2, 7], 100, ["uniform", "uniform", "uniform"], "u11", 4)
+    Y = CooTensor([20, 1, 7], np.stack([Y.idx[0], np.zeros_like(Y.idx[1]), Y.idx[2]]), Y.val)
     check_vs_oracle(run(ctx, X, Y, [2], [0]), X, Y, [2], [0])
 
 
