@@ -381,6 +381,7 @@ def ours_arm(args, world, rank, local, dist):
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "heavy_windows": s0["heavy_windows"], "heavy_rows": s0["heavy_rows"], "rows": s0["rows"],
             "stage_ms": {k: s0[k] for k in ("t_linearize_ms", "t_sort_ms", "t_match_ms", "t_plan_ms",
                                              "t_contract_ms", "t_total_ms")},
         }

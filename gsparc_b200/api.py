@@ -69,7 +69,8 @@ class Stats(ctypes.Structure):
                 ("t_plan_ms", ctypes.c_double), ("t_contract_ms", ctypes.c_double),
                 ("t_output_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
                 ("bytes_h2d", ctypes.c_uint64), ("bytes_d2h", ctypes.c_uint64),
-                ("kernel_launches", ctypes.c_uint64), ("t_numeric_kernel_ms", ctypes.c_double)]
+                ("kernel_launches", ctypes.c_uint64), ("t_numeric_kernel_ms", ctypes.c_double),
+                ("heavy_windows", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -183,7 +183,7 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
     DBuf<uint32_t> d_heavy(A, h_heavy.size(), s), d_light(A, h_light.size(), s);
     h2d(d_heavy.get(), h_heavy.data(), h_heavy.size(), s);
     h2d(d_light.get(), h_light.data(), h_light.size(), s);
-    DBuf<uint32_t> cursor(A, nx, s);
+    DBuf<uint32_t> cursor(A, nx, s), pend(A, nx, s);
     DBuf<uint32_t> row_nnz(A, nrows, s);
     DBuf<uint64_t> row_off(A, nrows + 1, s);
     GS_CUDA(cudaMemsetAsync(row_nnz.get(), 0, 4 * (nrows ? nrows : 1), s));
@@ -201,6 +201,8 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
     aa.y_nfbits = LY.nfbits;
     aa.work_counter = ctx->d_flag + 1;
     aa.cursor = cursor;
+    aa.pend = pend;
+    aa.ncols = (uint32_t)yp.ncols;
     aa.row_nnz = row_nnz;
     aa.row_off = row_off;
     aa.err = ctx->d_flag;
@@ -336,8 +338,11 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
         t_out += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     tl.mark(5, s);
-    d2h(&herr, ctx->d_flag, 1, s);
+    unsigned int hflags[4] = {0, 0, 0, 0};
+    d2h(hflags, ctx->d_flag, 4, s);
     GS_CUDA(cudaStreamSynchronize(s));
+    herr = hflags[0];
+    st.heavy_windows = hflags[2];
     GS_REQUIRE(!(herr & 2u), GSPARC_EINTERNAL, "light unit over capacity");
     GS_REQUIRE(!(herr & 4u), GSPARC_EINTERNAL, "numeric pass wrote past its chunk (symbolic count mismatch)");
 

@@ -76,7 +76,9 @@ struct AccArgs {
     const uint32_t *units;     // light: pairs (r0, r1); heavy: row ids
     uint32_t nunits;
     unsigned int *work_counter;
-    uint32_t *cursor;          // [nx] scratch (heavy path)
+    uint32_t *cursor;          // [nx] scratch (heavy path): next unprocessed Y entry per run
+    uint32_t *pend;            // [nx] scratch (heavy path): end of the run's part in the window
+    uint32_t ncols;            // distinct Y free indices (column ranks are < ncols)
     // symbolic output
     uint32_t *row_nnz;         // [nrows]
     // numeric output
@@ -88,8 +90,12 @@ struct AccArgs {
     unsigned int *err;
 };
 
-constexpr int kHeavyW = 8192;      // dense window width (columns)
 constexpr int kHeavyThreads = 512;
+constexpr int kHeavyRW = 1 << 17;  // column ranks covered by one window's touched bitmap
+constexpr int kHeavyCap = 7168;    // output slots (compensated accumulators) per window
+                                   // (sized so two CTAs fit one SM's shared memory)
+constexpr int kHeavyMaxRuns = 512;   // runs flattened per batch
+constexpr int kGallopWarpRuns = 64;  // up to this many runs per batch: one warp per run search
 constexpr int kLightCap = 4096;    // on-chip ESC capacity (products per unit)
 constexpr int kLightThreads = 512;
 constexpr uint64_t kLightRowMax = 1024;   // rows with at most this many products are light

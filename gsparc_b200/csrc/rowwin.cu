@@ -1,0 +1,481 @@
+// rowwin.cu -- windowed accumulation of heavy output rows.
+//
+// One CTA owns one output row (all products of one X free index).  The row's
+// products are the matched Y runs of its X nonzeros; every run is sorted by
+// column rank.  The CTA sweeps the column-rank axis in windows [R0, R0+rw):
+//
+//  A. each run's part inside the window is found by a search from the run's
+//     cursor (a warp per run with a 32-way fan-out when runs are few, a thread
+//     per run when they are many); parts that are empty are dropped;
+//  B. a block scan flattens the remaining parts into one index space, so every
+//     thread gets the same share of entries however uneven the runs are; a
+//     warp maps its 32 entries to parts with a 5-step shuffle search;
+//  1. touched columns are marked in a shared bitmap;
+//  2. a word-wise prefix of the bitmap turns each touched column into a dense
+//     output slot (slot = prefix[word] + popcount of lower bits), so the output
+//     of the window is already in column order;
+//  3. (numeric) every product is added into its slot with compensated FP32:
+//     the hardware add returns the old value, from which TwoSum rebuilds the
+//     exact rounding error of that add; errors (and the product's own fma
+//     error) accumulate in a second word;
+//  4. (numeric) a slot -> column table is built from the bitmap (a thread per
+//     word), then every warp writes 32 consecutive slots per step.
+//
+// The window width adapts to the row's density so a window holds at most
+// kHeavyCap outputs; a window that overflows is cut at the kHeavyCap-th
+// touched column and the rest is taken by the next window.  The symbolic pass
+// (steps A, B, 1, 2 with the widest window) counts each row's outputs.
+#include "blockops.cuh"
+#include "kernels.cuh"
+
+namespace gs {
+
+namespace {
+using namespace dev;
+
+constexpr int T = kHeavyThreads;
+constexpr int NWARPS = T / 32;
+constexpr int RW = kHeavyRW;
+constexpr int NWORDS = RW / 32;
+constexpr int CAP = kHeavyCap;
+constexpr int MAXR = kHeavyMaxRuns;
+constexpr int WPN = (NWORDS > CAP ? NWORDS : CAP) + 4;  // word prefix, later the slot -> column table
+constexpr int WPT_MAX = (NWORDS + T - 1) / T;
+constexpr uint32_t INF = 0xffffffffu;
+constexpr uint32_t FULL = 0xffffffffu;
+static_assert(MAXR <= 2 * T, "run batch is scanned two per thread");
+
+// First index in [p, e) whose rank is >= lim (e if none); *first_rank gets
+// that entry's rank (INF if none).  All lanes of the warp call it with the
+// same arguments.  Exponential search with a 32-way fan-out per step: the
+// stride grows 32x while the window still holds the next 32 probes, then
+// narrows 32x per step, so a part of length L costs about 2*log32(L) loads.
+__device__ __forceinline__ uint32_t warp_gallop(const uint32_t *__restrict__ rank, uint32_t p, uint32_t e,
+                                                uint32_t lim, uint32_t *first_rank) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t base = p;
+    uint64_t s = 32;
+    for (;;) {
+        const uint64_t q = base + s * (lane + 1) - 1;
+        const uint32_t r = q < e ? rank[q] : INF;
+        const uint32_t bal = __ballot_sync(FULL, r >= lim);
+        if (bal) {
+            base += s * (uint64_t)(__ffs(bal) - 1);
+            break;
+        }
+        base += s * 32;
+        if (s < (1ull << 25)) s <<= 5;
+    }
+    // entries [p, base) are < lim and the entry at base + s - 1 is not
+    uint32_t fr = INF;
+    while (s > 1) {
+        s >>= 5;
+        const uint64_t q = base + s * (lane + 1) - 1;
+        const uint32_t r = q < e ? rank[q] : INF;
+        const uint32_t bal = __ballot_sync(FULL, r >= lim);
+        const int f = __ffs(bal) - 1;
+        base += s * (uint64_t)f;
+        if (s == 1) fr = __shfl_sync(FULL, r, f);
+    }
+    *first_rank = fr;
+    return base < e ? (uint32_t)base : e;
+}
+
+// Same search done by one thread: probe p, p+1, p+3, p+7, ... until a rank
+// >= lim (or e), then bisect the last gap.  Cheap when the part is short.
+__device__ __forceinline__ uint32_t thread_gallop(const uint32_t *__restrict__ rank, uint32_t p, uint32_t e,
+                                                  uint32_t lim, uint32_t *first_rank) {
+    uint32_t r = rank[p];
+    if (r >= lim) {
+        *first_rank = r;
+        return p;
+    }
+    uint32_t lo = p, hi = e, fr = INF, step = 1;  // rank[lo] < lim; hi == e or rank[hi] >= lim
+    for (;;) {
+        const uint64_t q = (uint64_t)lo + step;
+        if (q >= e) break;
+        const uint32_t rq = rank[q];
+        if (rq >= lim) {
+            hi = (uint32_t)q;
+            fr = rq;
+            break;
+        }
+        lo = (uint32_t)q;
+        step <<= 1;
+    }
+    while (hi - lo > 1) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        const uint32_t rm = rank[mid];
+        if (rm >= lim) {
+            hi = mid;
+            fr = rm;
+        } else {
+            lo = mid;
+        }
+    }
+    *first_rank = fr;
+    return hi;
+}
+
+// In-place exclusive scan of v[0..n) (n <= 2*T); v[n] gets the total.
+__device__ __forceinline__ void block_scan_inplace(uint32_t *v, uint32_t n, uint32_t *s_tmp) {
+    const uint32_t i0 = 2u * threadIdx.x, i1 = i0 + 1u;
+    const uint32_t a = i0 < n ? v[i0] : 0u;
+    const uint32_t b = i1 < n ? v[i1] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_excl_scan_u32<T>(a + b, s_tmp, &total);
+    if (i0 < n) v[i0] = ex;
+    if (i1 < n) v[i1] = ex + a;
+    if (threadIdx.x == 0) v[n] = total;
+    __syncthreads();
+}
+
+// The parts of runs [0, nb) sit uncompacted in the seg arrays (seg_off holds
+// lengths).  Drop empty parts, then turn lengths into an exclusive prefix with
+// the total at seg_off[ns].  Returns ns, the number of non-empty parts.
+__device__ __forceinline__ uint32_t compact_parts(uint32_t nb, uint32_t *seg_start, uint32_t *seg_off,
+                                                  uint32_t *seg_run, uint32_t *seg_cut, uint32_t *s_tmp) {
+    const uint32_t k0 = 2u * threadIdx.x, k1 = k0 + 1u;
+    uint32_t s0 = 0, l0 = 0, r0 = 0, c0 = 0, s1 = 0, l1 = 0, r1 = 0, c1 = 0;
+    if (k0 < nb) { s0 = seg_start[k0]; l0 = seg_off[k0]; r0 = seg_run[k0]; c0 = seg_cut[k0]; }
+    if (k1 < nb) { s1 = seg_start[k1]; l1 = seg_off[k1]; r1 = seg_run[k1]; c1 = seg_cut[k1]; }
+    const uint32_t f0 = (k0 < nb && l0) ? 1u : 0u, f1 = (k1 < nb && l1) ? 1u : 0u;
+    uint32_t ns;
+    const uint32_t at = block_excl_scan_u32<T>(f0 + f1, s_tmp, &ns);  // all reads done before it returns
+    if (f0) { seg_start[at] = s0; seg_off[at] = l0; seg_run[at] = r0; seg_cut[at] = c0; }
+    if (f1) { seg_start[at + f0] = s1; seg_off[at + f0] = l1; seg_run[at + f0] = r1; seg_cut[at + f0] = c1; }
+    __syncthreads();
+    block_scan_inplace(seg_off, ns, s_tmp);
+    return ns;
+}
+
+// Flattened walk over the non-empty parts seg[0..ns): every entry idx of every
+// part is visited once, entries spread evenly over the CTA's warps.  Each warp
+// step takes ILP chunks of 32 consecutive entries; load(k, idx, item) runs for
+// all of them before body(k, idx, item) runs for any, so a warp keeps ILP
+// independent memory loads in flight.  Lanes find their part with a shuffle
+// search over the next 32 part boundaries (parts are non-empty, so at most 32
+// of them start inside a chunk of 32 entries).
+constexpr int ILP = 4;
+
+template <class Item, class Load, class Body>
+__device__ __forceinline__ void flat_for(const uint32_t *seg_start, const uint32_t *seg_off, uint32_t ns,
+                                         Load &&load, Body &&body) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tot = seg_off[ns];
+    uint32_t k = 0;  // warp-uniform: the part holding the chunk's first entry
+    for (uint32_t base = warp * 32u * ILP; base < tot; base += NWARPS * 32u * ILP) {
+        uint32_t kk[ILP], idx[ILP];
+        bool ok[ILP];
+#pragma unroll
+        for (int u = 0; u < ILP; ++u) {
+            const uint32_t cb = base + 32u * u;
+            // seg_off is increasing, so "seg_off[j] <= cb" holds for a prefix of j
+            for (;;) {
+                const uint32_t j = k + 1 + lane;
+                const bool le = j < ns && seg_off[j] <= cb;
+                const uint32_t n = __popc(__ballot_sync(FULL, le));
+                k += n;
+                if (n < 32) break;
+            }
+            const uint32_t t = cb + lane;
+            const uint32_t bj = (k + 1 + lane <= ns) ? seg_off[k + 1 + lane] : INF;
+            // c = number of part boundaries in (cb, t]; every part holds at least
+            // one entry, so at most 31 of them fall inside the chunk and the
+            // 5-step lifting over the 32 loaded boundaries is exact
+            uint32_t c = 0;
+#pragma unroll
+            for (uint32_t step = 16; step >= 1; step >>= 1) {
+                const uint32_t b = __shfl_sync(FULL, bj, c + step - 1);
+                if (b <= t) c += step;
+            }
+            const uint32_t q = k + c;
+            ok[u] = t < tot && q < ns;  // q < ns always holds when t < tot; checked, not trusted
+            kk[u] = q;
+            idx[u] = ok[u] ? seg_start[q] + (t - seg_off[q]) : 0u;
+        }
+        Item it[ILP];
+#pragma unroll
+        for (int u = 0; u < ILP; ++u)
+            if (ok[u]) load(kk[u], idx[u], it[u]);
+#pragma unroll
+        for (int u = 0; u < ILP; ++u)
+            if (ok[u]) body(kk[u], idx[u], it[u]);
+    }
+}
+
+struct RankItem {
+    uint32_t r;
+};
+struct ProdItem {
+    uint32_t r;
+    float xv, yv;
+};
+
+template <bool NUMERIC>
+__global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t *bits = reinterpret_cast<uint32_t *>(smem_raw);  // [NWORDS]
+    uint32_t *wp = bits + NWORDS;                              // [WPN]
+    uint32_t *seg_start = wp + WPN;                            // [MAXR]
+    uint32_t *seg_off = seg_start + MAXR;                      // [MAXR + 4]
+    uint32_t *seg_run = seg_off + MAXR + 4;                    // [MAXR]
+    uint32_t *seg_cut = seg_run + MAXR;                        // [MAXR]
+    float *hi = reinterpret_cast<float *>(seg_cut + MAXR);     // [CAP]   (numeric)
+    float *lo = hi + CAP;                                      // [CAP]   (numeric)
+    uint32_t *ocol = wp;  // step 4 reuses the word prefix as the slot -> column table
+    __shared__ uint32_t s_tmp[33];
+    __shared__ uint32_t s_unit;
+    __shared__ uint32_t s_cut;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+
+    for (int i = tid; i < NWORDS; i += T) bits[i] = 0;
+    if (NUMERIC)
+        for (int i = tid; i < CAP; i += T) hi[i] = lo[i] = 0.f;
+    __syncthreads();
+
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(a.work_counter, 1u);
+        __syncthreads();
+        const uint32_t u = s_unit;
+        if (u >= a.nunits) break;
+        const uint32_t row = a.units[u];
+        const uint32_t xs = a.row_start[row], xe = a.row_start[row + 1];
+        const uint64_t xf_hi = shl(a.row_xf[row], a.y_nfbits);
+
+        uint32_t mymin = INF;
+        for (uint32_t i = xs + tid; i < xe; i += T) {
+            const uint32_t p = a.pos[i];
+            a.cursor[i] = p;
+            if (a.cnt[i]) mymin = min(mymin, a.yrank[p]);
+        }
+        uint32_t R0 = block_min_u32<T>(mymin, s_tmp);
+
+        // initial window width from the row's density (products vs columns)
+        uint32_t rw = RW;
+        if (NUMERIC) {
+            const uint64_t P = a.xprefix[xe] - a.xprefix[xs];
+            const uint64_t est = (uint64_t)CAP * a.ncols / (P ? P : 1);
+            const uint64_t clamped = est < 32ull ? 32ull : (est > (uint64_t)RW ? (uint64_t)RW : est);
+            rw = (uint32_t)clamped & ~31u;
+        }
+        uint64_t out_pos = NUMERIC ? (a.row_off[row] - a.chunk_base) : 0;
+        uint32_t row_total = 0;
+        const bool one_batch = xe - xs <= (uint32_t)MAXR;  // parts from step A stay in place
+
+        while (R0 != INF) {
+            const uint32_t lim = R0 + rw;  // ranks < 2^31: no wrap
+            const uint32_t nwu = rw >> 5;  // bitmap words in use
+            uint32_t nextmin = INF;
+            uint32_t ns = 0;
+
+            // ---- A, B, 1: parts of every run inside the window, marked in the bitmap
+            for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
+                const uint32_t nb = min((uint32_t)MAXR, xe - b0);
+                if (nb <= (uint32_t)kGallopWarpRuns) {
+                    // few runs, long parts: one warp per run, 32-way fan-out search
+                    for (uint32_t k = warp; k < nb; k += NWARPS) {
+                        const uint32_t i = b0 + k;
+                        const uint32_t p = a.cursor[i];
+                        const uint32_t e = a.pos[i] + a.cnt[i];
+                        uint32_t pe = p, fr = INF;
+                        if (p < e) pe = warp_gallop(a.yrank, p, e, lim, &fr);
+                        if (lane == 0) {
+                            seg_start[k] = p;
+                            seg_off[k] = pe - p;
+                            seg_run[k] = i;
+                            seg_cut[k] = pe;
+                            a.pend[i] = pe;
+                        }
+                        nextmin = min(nextmin, fr);
+                    }
+                } else {
+                    // many runs, short parts: one thread per run, doubling then bisection
+                    for (uint32_t k = tid; k < nb; k += T) {
+                        const uint32_t i = b0 + k;
+                        const uint32_t p = a.cursor[i];
+                        const uint32_t e = a.pos[i] + a.cnt[i];
+                        uint32_t pe = p, fr = INF;
+                        if (p < e) pe = thread_gallop(a.yrank, p, e, lim, &fr);
+                        seg_start[k] = p;
+                        seg_off[k] = pe - p;
+                        seg_run[k] = i;
+                        seg_cut[k] = pe;
+                        a.pend[i] = pe;
+                        nextmin = min(nextmin, fr);
+                    }
+                }
+                __syncthreads();
+                ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
+                flat_for<RankItem>(
+                    seg_start, seg_off, ns,
+                    [&](uint32_t, uint32_t idx, RankItem &it) { it.r = a.yrank[idx]; },
+                    [&](uint32_t, uint32_t, const RankItem &it) {
+                        const uint32_t c = it.r - R0;
+                        const uint32_t m = 1u << (c & 31);
+                        if (!(bits[c >> 5] & m)) atomicOr(&bits[c >> 5], m);
+                    });
+                __syncthreads();
+            }
+
+            // ---- 2: word prefix of the bitmap
+            // words in use are split in blocks of wpt consecutive words per thread
+            const uint32_t wpt = (nwu + T - 1) / T;
+            const uint32_t w0 = (uint32_t)tid * wpt;
+            const uint32_t w1 = min(w0 + wpt, nwu);
+            uint32_t loc = 0;
+            for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
+            uint32_t Dw;
+            uint32_t run = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
+            for (uint32_t w = w0; w < w1; ++w) {
+                wp[w] = run;
+                run += __popc(bits[w]);
+            }
+
+            if (!NUMERIC) {
+                row_total += Dw;
+                for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
+                for (uint32_t i = xs + tid; i < xe; i += T) a.cursor[i] = a.pend[i];
+                R0 = block_min_u32<T>(nextmin, s_tmp);
+                continue;
+            }
+
+            // ---- numeric: cut the window at the CAP-th touched column if needed
+            const bool over = Dw > (uint32_t)CAP;
+            uint32_t R1 = lim, outputs = Dw;
+            if (over) {
+                for (uint32_t w = w0; w < w1; ++w) {
+                    if (wp[w] <= (uint32_t)CAP && (uint32_t)CAP < wp[w] + __popc(bits[w])) {
+                        const uint32_t b = __fns(bits[w], 0u, (int)((uint32_t)CAP - wp[w] + 1));
+                        s_cut = R0 + 32u * w + b;
+                    }
+                }
+                __syncthreads();
+                R1 = s_cut;
+                outputs = CAP;
+            }
+            __syncthreads();
+
+            // ---- 3: accumulate every product of the window into its slot
+            for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
+                const uint32_t nb = min((uint32_t)MAXR, xe - b0);
+                if (!one_batch) {
+                    for (uint32_t k = tid; k < nb; k += T) {
+                        const uint32_t i = b0 + k;
+                        const uint32_t p = a.cursor[i];
+                        const uint32_t pe = a.pend[i];
+                        seg_start[k] = p;
+                        seg_off[k] = pe - p;
+                        seg_run[k] = i;
+                        seg_cut[k] = pe;
+                    }
+                    __syncthreads();
+                    ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
+                }
+                flat_for<ProdItem>(
+                    seg_start, seg_off, ns,
+                    [&](uint32_t k, uint32_t idx, ProdItem &it) {
+                        it.r = a.yrank[idx];
+                        it.yv = a.yval[idx];
+                        it.xv = a.xval[seg_run[k]];
+                    },
+                    [&](uint32_t k, uint32_t idx, const ProdItem &it) {
+                        if (it.r < R1) {
+                            const uint32_t c = it.r - R0;
+                            const uint32_t w = c >> 5;
+                            const uint32_t slot = wp[w] + __popc(bits[w] & ((1u << (c & 31)) - 1u));
+                            const float pr = it.xv * it.yv;
+                            const float pe = fmaf(it.xv, it.yv, -pr);
+                            const float old = atomicAdd(&hi[slot], pr);
+                            float s, err;
+                            two_sum(old, pr, s, err);
+                            atomicAdd(&lo[slot], err + pe);
+                        } else {
+                            atomicMin(&seg_cut[k], idx);
+                        }
+                    });
+                __syncthreads();
+                for (uint32_t k = tid; k < ns; k += T) a.cursor[seg_run[k]] = seg_cut[k];
+                __syncthreads();
+            }
+
+            // ---- 4: slot -> column table, then coalesced writes of the window.
+            // The word prefix is read into registers before the table overwrites it.
+            {
+                uint32_t myw[WPT_MAX], myp[WPT_MAX];
+#pragma unroll
+                for (int q = 0; q < WPT_MAX; ++q) {
+                    const uint32_t w = w0 + q;
+                    myw[q] = w < w1 ? bits[w] : 0u;
+                    myp[q] = w < w1 ? wp[w] : 0u;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int q = 0; q < WPT_MAX; ++q) {
+                    uint32_t bw = myw[q];
+                    uint32_t slot = myp[q];
+                    const uint32_t cbase = R0 + 32u * (w0 + q);
+                    while (bw && slot < outputs) {
+                        ocol[slot++] = cbase + (uint32_t)(__ffs(bw) - 1);
+                        bw &= bw - 1;
+                    }
+                }
+                __syncthreads();
+                // The stores stream past L2 so the output does not evict the Y operand.
+                for (uint32_t q = tid; q < outputs; q += T) {
+                    const uint64_t o = out_pos + q;
+                    const float v = hi[q] + lo[q];
+                    if (o < a.out_cap) {
+                        __stcs(a.out_keys + o, (unsigned long long)(xf_hi | a.cols[ocol[q]]));
+                        __stcs(a.out_vals + o, v);
+                    } else {
+                        atomicOr(a.err, 4u);
+                    }
+                    hi[q] = 0.f;
+                    lo[q] = 0.f;
+                }
+            }
+            for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
+            if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
+            out_pos += outputs;
+            row_total += outputs;
+            if (over) {
+                rw = max(32u, (R1 - R0 + 31u) & ~31u);
+                __syncthreads();
+                R0 = R1;
+            } else {
+                if (Dw < (uint32_t)CAP / 4) rw = min((uint32_t)RW, rw * 2u);
+                R0 = block_min_u32<T>(nextmin, s_tmp);
+            }
+        }
+        if (!NUMERIC && tid == 0) a.row_nnz[row] = row_total;
+        __syncthreads();
+    }
+}
+
+size_t rowwin_smem(bool numeric) {
+    const size_t words = (size_t)NWORDS + WPN + MAXR + (MAXR + 4) + MAXR + MAXR;
+    return words * 4 + (numeric ? (size_t)CAP * 8 : 0);
+}
+
+}  // namespace
+
+int heavy_blocks_per_sm() { return 2; }
+
+void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s) {
+    if (a.nunits == 0) return;
+    const size_t sm = rowwin_smem(numeric);
+    if (numeric) {
+        GS_CUDA(cudaFuncSetAttribute(k_rowwin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_rowwin<true><<<grid, T, sm, s>>>(a);
+    } else {
+        GS_CUDA(cudaFuncSetAttribute(k_rowwin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_rowwin<false><<<grid, T, sm, s>>>(a);
+    }
+    count_launch();
+    GS_CUDA(cudaGetLastError());
+}
+
+}  // namespace gs

@@ -108,6 +108,7 @@ typedef struct {
     uint64_t bytes_h2d, bytes_d2h;
     uint64_t kernel_launches; /* this library's own kernels launched           */
     double t_numeric_kernel_ms; /* device time of the numeric accumulation kernels */
+    uint64_t heavy_windows;   /* column windows swept by the heavy-row accumulator */
 } gsparc_stats;
 
 /* ---- version / errors ---------------------------------------------------- */
