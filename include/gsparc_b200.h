@@ -210,6 +210,25 @@ gsparc_status gsparc_index_match(gsparc_ctx *ctx, uint64_t nx, const uint64_t *d
                                  int y_nfbits, uint64_t *d_pos, uint64_t *d_cnt,
                                  uint64_t *d_prefix, uint64_t *ir, void *stream);
 
+/* The same index match for callers that cannot allocate device memory: code
+ * running while a stream is captured into a CUDA graph, hosts whose own
+ * allocator owns the GPU's memory, paths that must not enter the driver's
+ * allocator.  It needs no context and calls no cudaMalloc/cudaFree or other
+ * allocating routine: its scratch (Y's run table and CUB's temporary storage)
+ * is one 64 MiB file-scope device array that every GPU loading the library
+ * holds until exit, enough for Y up to about 4.9 million keys; larger inputs
+ * return GSPARC_EINVAL with the limit in gsparc_last_error().  The first call
+ * on each device looks the array's address up (cudaGetSymbolAddress) with
+ * that device current: make it before any stream capture.  All calls on a
+ * device share the array, so calls that overlap on the GPU race and must be
+ * serialised by the caller; nothing is carried over between calls.
+ * No counterpart in the reference (its IndexMatch allocates from its pool,
+ * include/gsparc/indexMatch.cuh:270-286). */
+gsparc_status gsparc_index_match_noalloc(uint64_t nx, const uint64_t *d_xkeys, int x_ncbits,
+                                         uint64_t ny, const uint64_t *d_ykeys, int y_nfbits,
+                                         uint64_t *d_pos, uint64_t *d_cnt, uint64_t *d_prefix,
+                                         uint64_t *ir, void *stream);
+
 /* ---- verification digest of an output chunk ------------------------------ */
 /* Order-independent digest of n output nonzeros on the device: count, a sum
  * of mixed keys, how many neighbours are not strictly increasing, the first
