@@ -83,6 +83,7 @@ gsparc_status gsparc_ctx_create(int device, uint64_t budget, gsparc_ctx **out) {
             ctx->arena.init(device, budget);
             for (auto &e : ctx->ev) GS_CUDA(cudaEventCreate(&e));
             GS_CUDA(cudaMalloc(&ctx->d_flag, 64));
+            GS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
             GS_CUDA(cudaMemset(ctx->d_flag, 0, 64));
         } catch (...) {
             delete ctx;
@@ -100,6 +101,7 @@ gsparc_status gsparc_ctx_destroy(gsparc_ctx *ctx) {
         for (auto &e : ctx->ev)
             if (e) cudaEventDestroy(e);
         if (ctx->d_flag) cudaFree(ctx->d_flag);
+        if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         delete ctx;
     });
 }

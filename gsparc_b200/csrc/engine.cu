@@ -206,7 +206,8 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
     aa.row_nnz = row_nnz;
     aa.row_off = row_off;
     aa.err = ctx->d_flag;
-    const int gh = std::max(1, ctx->sm_count * heavy_blocks_per_sm());
+    const int ghs = std::max(1, ctx->sm_count * heavy_blocks_per_sm(false));
+    const int gh = std::max(1, ctx->sm_count * heavy_blocks_per_sm(true));
     const int gl = std::max(1, ctx->sm_count * light_blocks_per_sm());
 
     // ---- symbolic pass ----
@@ -219,7 +220,7 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
         b.units = d_heavy;
         b.nunits = (uint32_t)h_heavy.size();
         GS_CUDA(cudaMemsetAsync(ctx->d_flag + 1, 0, 4, s));
-        launch_heavy(b, false, std::min<int>(gh, (int)std::max<size_t>(1, b.nunits)), s);
+        launch_heavy(b, false, std::min<int>(ghs, (int)std::max<size_t>(1, b.nunits)), s);
     }
     exclusive_scan_u32_to_u64(A, row_nnz, row_off, nrows, s);
     std::vector<uint64_t> h_off(nrows + 1);
@@ -238,7 +239,7 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
     uint64_t cap = sink.max_chunk_nnz;
     if (cap == 0) {
         uint64_t avail = A.available();
-        cap = avail / 2 / 12;  // keep half the remaining budget for other work
+        cap = avail / 3 / 12;  // two chunk buffers (compute one, deliver the other), a third spare
         cap = std::min<uint64_t>(cap, 1ull << 31);
     }
     cap = std::max<uint64_t>(cap, 1);
@@ -268,13 +269,27 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
     }
     st.chunks = chunks.size();
 
-    DBuf<uint64_t> out_k(A, nnz_total ? cap : 1, s);
-    DBuf<float> out_v(A, nnz_total ? cap : 1, s);
+    // Two chunk buffers: chunk c+1 is computed on `s` while chunk c is handed to
+    // the sink (device->host copies run on a second stream, ordered after the
+    // chunk's kernels by an event).  A buffer is refilled only after its
+    // delivery returned, so no device-side wait is needed for reuse.
+    const int nbuf = chunks.size() > 1 ? 2 : 1;
+    DBuf<uint64_t> out_k[2];
+    DBuf<float> out_v[2];
+    for (int i = 0; i < nbuf; ++i) {
+        out_k[i].reset(A, nnz_total ? cap : 1, s);
+        out_v[i].reset(A, nnz_total ? cap : 1, s);
+    }
     double t_out = 0;
-    std::vector<cudaEvent_t> kev;
-    bool host_whole = sink.kind == GSPARC_SINK_HOST && sink.host_capacity >= nnz_total;
+    std::vector<cudaEvent_t> kev(2 * chunks.size(), nullptr);
+    for (auto &e : kev) GS_CUDA(cudaEventCreate(&e));
+    std::vector<DBuf<uint32_t>> unit_bufs(2 * chunks.size());
+    const bool host_whole = sink.kind == GSPARC_SINK_HOST && sink.host_capacity >= nnz_total;
+    cudaStream_t s2 = ctx->copy_stream;
 
-    for (const Chunk &c : chunks) {
+    auto enqueue = [&](size_t ci) {
+        const Chunk &c = chunks[ci];
+        const int bi = (int)(ci % nbuf);
         // per-chunk unit lists; heavy rows largest first
         std::vector<uint32_t> hh, hl;
         for (size_t u = c.u0; u < c.u1; ++u) {
@@ -282,53 +297,53 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
             else { hl.push_back(units[u].r0); hl.push_back(units[u].r1); }
         }
         std::sort(hh.begin(), hh.end(), [&](uint32_t a, uint32_t b) { return row_prod[a] > row_prod[b]; });
-        DBuf<uint32_t> dh(A, hh.size(), s), dl(A, hl.size(), s);
+        DBuf<uint32_t> &dh = unit_bufs[2 * ci], &dl = unit_bufs[2 * ci + 1];
+        dh.reset(A, hh.size(), s);
+        dl.reset(A, hl.size(), s);
         h2d(dh.get(), hh.data(), hh.size(), s);
         h2d(dl.get(), hl.data(), hl.size(), s);
         AccArgs b = aa;
         b.chunk_base = h_off[ra] + c.first;
-        b.out_keys = out_k;
-        b.out_vals = out_v;
+        b.out_keys = out_k[bi];
+        b.out_vals = out_v[bi];
         b.out_cap = c.n;
         b.units = dl;
         b.nunits = (uint32_t)(hl.size() / 2);
         GS_CUDA(cudaMemsetAsync(ctx->d_flag + 1, 0, 4, s));
-        kev.push_back(nullptr);
-        kev.push_back(nullptr);
-        GS_CUDA(cudaEventCreate(&kev[kev.size() - 2]));
-        GS_CUDA(cudaEventCreate(&kev[kev.size() - 1]));
-        GS_CUDA(cudaEventRecord(kev[kev.size() - 2], s));
+        GS_CUDA(cudaEventRecord(kev[2 * ci], s));
         launch_light(b, true, std::min<int>(gl, (int)std::max<size_t>(1, b.nunits)), s);
         b.units = dh;
         b.nunits = (uint32_t)hh.size();
         GS_CUDA(cudaMemsetAsync(ctx->d_flag + 1, 0, 4, s));
         launch_heavy(b, true, std::min<int>(gh, (int)std::max<size_t>(1, b.nunits)), s);
-        GS_CUDA(cudaEventRecord(kev.back(), s));
+        GS_CUDA(cudaEventRecord(kev[2 * ci + 1], s));
+    };
 
-        // deliver
+    auto deliver = [&](size_t ci) {
+        const Chunk &c = chunks[ci];
+        const int bi = (int)(ci % nbuf);
         auto t0 = std::chrono::steady_clock::now();
         if (sink.kind == GSPARC_SINK_DEVICE) {
-            GS_CUDA(cudaStreamSynchronize(s));
-            if (sink.on_chunk(sink.user, out_k.get(), out_v.get(), c.n, c.first, 1))
+            GS_CUDA(cudaEventSynchronize(kev[2 * ci + 1]));
+            if (sink.on_chunk(sink.user, out_k[bi].get(), out_v[bi].get(), c.n, c.first, 1))
                 fail(GSPARC_ECALLBACK, "output callback stopped the contraction");
         } else if (sink.kind == GSPARC_SINK_HOST) {
+            GS_CUDA(cudaStreamWaitEvent(s2, kev[2 * ci + 1], 0));
             if (host_whole) {
-                d2h(sink.host_keys + c.first, out_k.get(), c.n, s);
-                d2h(sink.host_vals + c.first, out_v.get(), c.n, s);
+                d2h(sink.host_keys + c.first, out_k[bi].get(), c.n, s2);
+                d2h(sink.host_vals + c.first, out_v[bi].get(), c.n, s2);
                 st.bytes_d2h += 12 * c.n;
-                if (sink.on_chunk) {
-                    GS_CUDA(cudaStreamSynchronize(s));
-                    if (sink.on_chunk(sink.user, sink.host_keys + c.first, sink.host_vals + c.first,
-                                      c.n, c.first, 0))
-                        fail(GSPARC_ECALLBACK, "output callback stopped the contraction");
-                }
+                GS_CUDA(cudaStreamSynchronize(s2));
+                if (sink.on_chunk && sink.on_chunk(sink.user, sink.host_keys + c.first, sink.host_vals + c.first,
+                                                   c.n, c.first, 0))
+                    fail(GSPARC_ECALLBACK, "output callback stopped the contraction");
             } else {
                 for (uint64_t off = 0; off < c.n; off += sink.host_capacity) {
-                    uint64_t n = std::min<uint64_t>(sink.host_capacity, c.n - off);
-                    d2h(sink.host_keys, out_k.get() + off, n, s);
-                    d2h(sink.host_vals, out_v.get() + off, n, s);
+                    const uint64_t n = std::min<uint64_t>(sink.host_capacity, c.n - off);
+                    d2h(sink.host_keys, out_k[bi].get() + off, n, s2);
+                    d2h(sink.host_vals, out_v[bi].get() + off, n, s2);
                     st.bytes_d2h += 12 * n;
-                    GS_CUDA(cudaStreamSynchronize(s));
+                    GS_CUDA(cudaStreamSynchronize(s2));
                     if (sink.on_chunk &&
                         sink.on_chunk(sink.user, sink.host_keys, sink.host_vals, n, c.first + off, 0))
                         fail(GSPARC_ECALLBACK, "output callback stopped the contraction");
@@ -336,6 +351,19 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
             }
         }
         t_out += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
+
+    try {
+        for (size_t ci = 0; ci < chunks.size(); ++ci) {
+            enqueue(ci);
+            if (ci >= 1) deliver(ci - 1);
+        }
+        if (!chunks.empty()) deliver(chunks.size() - 1);
+    } catch (...) {
+        cudaStreamSynchronize(s2);
+        cudaStreamSynchronize(s);
+        for (auto e : kev) cudaEventDestroy(e);
+        throw;
     }
     tl.mark(5, s);
     unsigned int hflags[4] = {0, 0, 0, 0};

@@ -128,6 +128,7 @@ struct gsparc_ctx {
     int sm_count = 148;
     cudaEvent_t ev[16] = {};
     unsigned int *d_flag = nullptr;  // device error / work counters
+    cudaStream_t copy_stream = nullptr;  // output chunk copies (non-blocking)
 };
 
 struct gsparc_tensor {

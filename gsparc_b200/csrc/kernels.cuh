@@ -103,7 +103,7 @@ constexpr uint64_t kLightUnitMax = 3072;  // products per light unit
 
 void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
 void launch_light(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
-int heavy_blocks_per_sm();
+int heavy_blocks_per_sm(bool numeric);
 int light_blocks_per_sm();
 
 // ---- misc ----

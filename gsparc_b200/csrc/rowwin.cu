@@ -462,7 +462,20 @@ size_t rowwin_smem(bool numeric) {
 
 }  // namespace
 
-int heavy_blocks_per_sm() { return 2; }
+// Resident CTAs per SM of each instantiation (registers and shared memory
+// decide: the symbolic pass needs no accumulators and fits more CTAs).
+int heavy_blocks_per_sm(bool numeric) {
+    int n = 0;
+    const size_t sm = rowwin_smem(numeric);
+    if (numeric) {
+        GS_CUDA(cudaFuncSetAttribute(k_rowwin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_rowwin<true>, T, sm));
+    } else {
+        GS_CUDA(cudaFuncSetAttribute(k_rowwin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_rowwin<false>, T, sm));
+    }
+    return n > 0 ? n : 1;
+}
 
 void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s) {
     if (a.nunits == 0) return;
