@@ -70,7 +70,7 @@ class Stats(ctypes.Structure):
                 ("t_output_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
                 ("bytes_h2d", ctypes.c_uint64), ("bytes_d2h", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("t_numeric_kernel_ms", ctypes.c_double),
-                ("heavy_windows", ctypes.c_uint64)]
+                ("heavy_windows", ctypes.c_uint64), ("stream_rows", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -83,8 +83,14 @@ EXPORTS = [
     "gsparc_ctx_destroy", "gsparc_ctx_memory", "gsparc_tensor_upload", "gsparc_tensor_free",
     "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
     "gsparc_free_host", "gsparc_layout", "gsparc_plan_shards", "gsparc_linearize",
-    "gsparc_sort_pairs", "gsparc_index_match", "gsparc_digest_chunk",
+    "gsparc_sort_pairs", "gsparc_index_match", "gsparc_digest_chunk", "gsparc_sptc_batch",
 ]
+
+
+class _Job(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("ncmodes", ctypes.c_int),
+                ("cx", ctypes.c_void_p), ("cy", ctypes.c_void_p), ("accum", ctypes.c_int),
+                ("sink", _Sink), ("stats", Stats), ("status", ctypes.c_int)]
 
 
 class Digest(ctypes.Structure):
@@ -127,6 +133,7 @@ def lib():
     L.gsparc_sort_pairs.argtypes = [P, U64, P, P, I, P]
     L.gsparc_index_match.argtypes = [P, U64, P, I, U64, P, I, P, P, P, P, P]
     L.gsparc_digest_chunk.argtypes = [P, P, U64, ctypes.POINTER(Digest), P]
+    L.gsparc_sptc_batch.argtypes = [P, P, I, U64, ctypes.POINTER(Stats), P]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype if name in (
             "gsparc_version", "gsparc_status_string", "gsparc_last_error") else (
@@ -373,6 +380,95 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
             keys = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0, np.uint64)
             vals = np.concatenate([p[2] for p in parts]) if parts else np.zeros(0, np.float32)
     return SpTCResult(int(st.nnz), int(st.ir_nnz), keys, vals, st.as_dict())
+
+
+def sptc_batch(ctx: Context, jobs, sink: str = "host", max_chunk_nnz: int = 0, stream: int = 0,
+               staging: int = 1 << 20, on_chunk=None, raise_on_error: bool = True):
+    """Many contractions in one call (gsparc_sptc_batch).
+
+    jobs: sequence of ``(X, Y, cx, cy)`` or ``(X, Y, cx, cy, accum)`` with
+    resident DeviceTensors.  sink: "host" (every job's Z copied into numpy
+    arrays through one shared staging buffer of ``staging`` entries),
+    "discard", or "device" (``on_chunk(job, keys_ptr, vals_ptr, n, first)``
+    with device pointers).  Returns ``(results, batch_stats)``; a failed job's
+    result has ``keys is None`` and its status in ``stats["status"]``.
+    """
+    n = len(jobs)
+    arr = (_Job * max(n, 1))()
+    keep = []
+    parts = [[] for _ in range(n)]
+    hk = hv = None
+    if sink == "host":
+        hk = np.zeros(staging, np.uint64)
+        hv = np.zeros(staging, np.float32)
+        keep += [hk, hv]
+
+        def _cbh(user, k, v, m, first, on_dev):
+            j = int(user or 0)
+            kk = np.ctypeslib.as_array(ctypes.cast(k, ctypes.POINTER(ctypes.c_uint64)), shape=(m,)).copy()
+            vv = np.ctypeslib.as_array(ctypes.cast(v, ctypes.POINTER(ctypes.c_float)), shape=(m,)).copy()
+            parts[j].append((first, kk, vv))
+            return 0
+        cb = CHUNK_FN(_cbh)
+    elif sink == "device":
+        if on_chunk is None:
+            raise ValueError("device sink needs on_chunk")
+
+        def _cbd(user, k, v, m, first, on_dev):
+            return int(bool(on_chunk(int(user or 0), k, v, m, first)))
+        cb = CHUNK_FN(_cbd)
+    elif sink == "discard":
+        cb = None
+    else:
+        raise ValueError(f"unknown sink {sink!r}")
+    if cb is not None:
+        keep.append(cb)
+    for j, job in enumerate(jobs):
+        X, Y, cx, cy = job[:4]
+        accum = job[4] if len(job) > 4 else ACCUM_AUTO
+        if len(cx) != len(cy):
+            raise ValueError("cx and cy must have the same length")
+        c1 = np.asarray(cx, np.int32)
+        c2 = np.asarray(cy, np.int32)
+        keep += [c1, c2]
+        J = arr[j]
+        J.x = X.handle
+        J.y = Y.handle
+        J.ncmodes = len(c1)
+        J.cx = c1.ctypes.data
+        J.cy = c2.ctypes.data
+        J.accum = int(accum)
+        J.sink.user = j
+        if sink == "host":
+            J.sink.kind = SINK_HOST
+            J.sink.host_keys = hk.ctypes.data
+            J.sink.host_vals = hv.ctypes.data
+            J.sink.host_capacity = staging
+            J.sink.on_chunk = cb
+        elif sink == "device":
+            J.sink.kind = SINK_DEVICE
+            J.sink.on_chunk = cb
+        else:
+            J.sink.kind = SINK_DISCARD
+    st = Stats()
+    rc = lib().gsparc_sptc_batch(ctx.handle, ctypes.cast(arr, ctypes.c_void_p), n, max_chunk_nnz,
+                                 ctypes.byref(st), ctypes.c_void_p(stream))
+    if rc != 0 and raise_on_error:
+        _check(rc, "sptc_batch")
+    results = []
+    for j in range(n):
+        J = arr[j]
+        d = J.stats.as_dict()
+        d["status"] = int(J.status)
+        keys = vals = None
+        if J.status == 0 and sink == "host":
+            ps = sorted(parts[j], key=lambda p: p[0])
+            keys = np.concatenate([p[1] for p in ps]) if ps else np.zeros(0, np.uint64)
+            vals = np.concatenate([p[2] for p in ps]) if ps else np.zeros(0, np.float32)
+        results.append(SpTCResult(int(J.stats.nnz), int(J.stats.ir_nnz), keys, vals, d))
+    bd = st.as_dict()
+    bd["status"] = int(rc)
+    return results, bd
 
 
 def SpTC(X: CooTensor, Y: CooTensor, cx: Sequence[int], cy: Sequence[int],

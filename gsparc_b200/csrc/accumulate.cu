@@ -171,7 +171,11 @@ __global__ void __launch_bounds__(kLightThreads) k_light(AccArgs a) {
             } while (e < P && key[e] == k);
             const uint64_t o = a.row_off[row] - a.chunk_base + rank_in_row;
             if (o < a.out_cap) {
-                a.out_keys[o] = shl(a.row_xf[row], a.y_nfbits) | a.cols[(uint32_t)k];
+                int y_nfbits;
+                const uint64_t *cols;
+                uint32_t ncols;
+                row_job_params(a, row, y_nfbits, cols, ncols);
+                a.out_keys[o] = shl(a.row_xf[row], y_nfbits) | cols[(uint32_t)k];
                 a.out_vals[o] = s + c;
             } else {
                 atomicOr(a.err, 4u);

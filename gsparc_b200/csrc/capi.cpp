@@ -195,6 +195,15 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
     });
 }
 
+gsparc_status gsparc_sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz,
+                                gsparc_stats *stats, void *stream) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        DeviceScope ds(ctx->device);
+        gs::sptc_batch(ctx, jobs, njobs, max_chunk_nnz, stats, (cudaStream_t)stream);
+    });
+}
+
 gsparc_status gsparc_read_tns(const char *path, int nthreads, int *order, uint64_t *dims, uint64_t *nnz,
                               uint64_t **idx, float **val) {
     return guard([&] {

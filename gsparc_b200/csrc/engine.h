@@ -11,6 +11,10 @@ void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int n
           const int *cy, int accum, int shard, int nshards, const gsparc_sink *sink,
           gsparc_stats *st, cudaStream_t s);
 
+// Many contractions as one (batch.cu).
+void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st,
+                cudaStream_t s);
+
 void plan_shards(const uint64_t *row_prod, uint64_t nrows, int nshards, uint64_t *bounds);
 
 // .tns text I/O (tns_io.cpp)

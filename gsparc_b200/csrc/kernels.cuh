@@ -59,7 +59,18 @@ void match_x(Arena &a, const uint64_t *xkeys, uint64_t nx, int x_ncbits, const Y
              XMatch &out, cudaStream_t s);
 
 // ---- accumulation ----
+// Per-job constants of a batch (gsparc_sptc_batch): rows of all jobs share
+// the arrays below, each row knows its job.
+struct BatchJob {
+    int y_nfbits;       // the job's Y free bits (output key = x_f << y_nfbits | y_f)
+    uint32_t ncols;     // the job's distinct Y free indices
+    uint64_t cols_off;  // where the job's distinct Y free indices start in `cols`
+};
+
 struct AccArgs {
+    // batch: job of every row (null for a single contraction) and job table
+    const uint16_t *row_job;
+    const BatchJob *jobs;
     // X side
     const uint32_t *row_start;
     const uint64_t *row_xf;
@@ -72,8 +83,12 @@ struct AccArgs {
     const float *yval;
     const uint64_t *cols;
     int y_nfbits;
+    // single-run rows (stream path): the matched X nonzero of every such row,
+    // and the product prefix over the listed rows (nunits + 1 entries)
+    const uint32_t *row_xi;
+    const uint64_t *sprefix;
     // work
-    const uint32_t *units;     // light: pairs (r0, r1); heavy: row ids
+    const uint32_t *units;     // light: pairs (r0, r1); heavy and stream: row ids
     uint32_t nunits;
     unsigned int *work_counter;
     uint32_t *cursor;          // [nx] scratch (heavy path): next unprocessed Y entry per run
@@ -101,7 +116,25 @@ constexpr int kLightThreads = 512;
 constexpr uint64_t kLightRowMax = 1024;   // rows with at most this many products are light
 constexpr uint64_t kLightUnitMax = 3072;  // products per light unit
 
+// Output-key width and column table of the job that owns `row`.
+__device__ __forceinline__ void row_job_params(const AccArgs &a, uint32_t row, int &y_nfbits,
+                                               const uint64_t *&cols, uint32_t &ncols) {
+    if (a.row_job) {
+        const BatchJob j = a.jobs[a.row_job[row]];
+        y_nfbits = j.y_nfbits;
+        cols = a.cols + j.cols_off;
+        ncols = j.ncols;
+    } else {
+        y_nfbits = a.y_nfbits;
+        cols = a.cols;
+        ncols = a.ncols;
+    }
+}
+
 void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
+// numeric pass of single-run rows (their symbolic count is their product count)
+void launch_stream(const AccArgs &a, int grid, cudaStream_t s);
+int stream_blocks_per_sm();
 void launch_light(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
 int heavy_blocks_per_sm(bool numeric);
 int light_blocks_per_sm();

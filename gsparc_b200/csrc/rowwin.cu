@@ -243,7 +243,11 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         if (u >= a.nunits) break;
         const uint32_t row = a.units[u];
         const uint32_t xs = a.row_start[row], xe = a.row_start[row + 1];
-        const uint64_t xf_hi = shl(a.row_xf[row], a.y_nfbits);
+        int y_nfbits;
+        const uint64_t *cols;
+        uint32_t ncols;
+        row_job_params(a, row, y_nfbits, cols, ncols);
+        const uint64_t xf_hi = shl(a.row_xf[row], y_nfbits);
 
         uint32_t mymin = INF;
         for (uint32_t i = xs + tid; i < xe; i += T) {
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         uint32_t rw = RW;
         if (NUMERIC) {
             const uint64_t P = a.xprefix[xe] - a.xprefix[xs];
-            const uint64_t est = (uint64_t)CAP * a.ncols / (P ? P : 1);
+            const uint64_t est = (uint64_t)CAP * ncols / (P ? P : 1);
             const uint64_t clamped = est < 32ull ? 32ull : (est > (uint64_t)RW ? (uint64_t)RW : est);
             rw = (uint32_t)clamped & ~31u;
         }
@@ -428,7 +432,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                     const uint64_t o = out_pos + q;
                     const float v = hi[q] + lo[q];
                     if (o < a.out_cap) {
-                        __stcs(a.out_keys + o, (unsigned long long)(xf_hi | a.cols[ocol[q]]));
+                        __stcs(a.out_keys + o, (unsigned long long)(xf_hi | cols[ocol[q]]));
                         __stcs(a.out_vals + o, v);
                     } else {
                         atomicOr(a.err, 4u);

@@ -29,6 +29,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
 from typing import Callable, List, Optional, Sequence
 
 import numpy as np
@@ -199,16 +200,24 @@ def dense_acc(scale: float = 1.0, seed: int = 2):
     return X, Y, [1, 2], [0, 1]
 
 
+def _make_pair(args):
+    dx, dy, nnz_x, nnz_y, ox, oy, s, sx = args[:8]
+    X = make_tensor(dx, nnz_x, [("zipf", s)] * ox, "u11", sx)
+    Y = make_tensor(dy, nnz_y, [("zipf", s)] * oy, "u11", sx + 1)
+    return X, Y
+
+
 def batched_instances(count: int = 256, seed: int = 3, max_nnz: int = 1_000_000,
-                      max_out_bits: int = 64):
+                      max_out_bits: int = 64, workers: int = 0):
     """Mixed instances: orders 3-4, modes log-uniform 64..100k, nnz log-uniform
     1e3..max_nnz, 1-2 contract modes, Zipf s in [1.0,1.4], U[-1,1).  Instances
-    whose output key would need more than ``max_out_bits`` bits are redrawn."""
+    whose output key would need more than ``max_out_bits`` bits are redrawn.
+    The tensors are drawn in ``workers`` spawned processes (0: one per core,
+    up to 32); every instance has its own seed, so the result does not depend
+    on the number of workers."""
     rng = np.random.default_rng(seed)
-    out = []
-    k = 0
-    while len(out) < count:
-        k += 1
+    params = []
+    while len(params) < count:
         ox = int(rng.integers(3, 5))
         oy = int(rng.integers(3, 5))
         nc = int(rng.integers(1, 3))
@@ -230,11 +239,21 @@ def batched_instances(count: int = 256, seed: int = 3, max_nnz: int = 1_000_000,
         nnz_x = int(min(nnz_x, cap_x // 4))
         nnz_y = int(min(nnz_y, cap_y // 4))
         sx = int(rng.integers(0, 2**31))
-        X = make_tensor(dx, nnz_x, [("zipf", s)] * ox, "u11", sx)
-        Y = make_tensor(dy, nnz_y, [("zipf", s)] * oy, "u11", sx + 1)
-        cx = list(range(ox - nc, ox))
-        cy = list(range(nc))
-        out.append((X, Y, cx, cy))
+        params.append((dx, dy, nnz_x, nnz_y, ox, oy, s, sx, nc))
+    if workers == 0:
+        workers = min(32, os.cpu_count() or 1)
+    total = sum(p[2] + p[3] for p in params)
+    if workers > 1 and total > 2_000_000:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        with cf.ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            pairs = list(ex.map(_make_pair, params, chunksize=1))
+    else:
+        pairs = [_make_pair(p) for p in params]
+    out = []
+    for p, (X, Y) in zip(params, pairs):
+        ox, nc = p[4], p[8]
+        out.append((X, Y, list(range(ox - nc, ox)), list(range(nc))))
     return out
 
 

@@ -109,6 +109,7 @@ typedef struct {
     uint64_t kernel_launches; /* this library's own kernels launched           */
     double t_numeric_kernel_ms; /* device time of the numeric accumulation kernels */
     uint64_t heavy_windows;   /* column windows swept by the heavy-row accumulator */
+    uint64_t stream_rows;     /* rows with one matched run, copied without accumulation */
 } gsparc_stats;
 
 /* ---- version / errors ---------------------------------------------------- */
@@ -157,6 +158,35 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
                                 int ncmodes, const int *cx, const int *cy, int accum,
                                 int shard, int nshards,
                                 const gsparc_sink *sink, gsparc_stats *stats, void *stream);
+
+/* One contraction of a batch: the arguments of gsparc_sptc plus per-job
+ * results. */
+typedef struct {
+    const gsparc_tensor *x, *y;
+    int ncmodes;
+    const int *cx, *cy;
+    int accum;             /* GSPARC_ACCUM_*                                   */
+    gsparc_sink sink;      /* this job's output; `first` counts from the job's
+                            * first output nonzero.  max_chunk_nnz caps the
+                            * pieces handed to a DEVICE sink's callback.      */
+    gsparc_stats stats;    /* out: this job's counts; stage times are the
+                            * batch's (the job's latency)                     */
+    gsparc_status status;  /* out: GSPARC_OK or why this job failed           */
+} gsparc_job;
+
+/* Many independent contractions as one.  The reference runs gsparc::SpTC
+ * (include/gsparc/sptc.cuh:16-360) once per contraction from main.cu:293-376;
+ * here every job's keys carry the job id in their top bits, so a group of
+ * jobs shares one linearise, one sort per side, one match and one symbolic +
+ * one numeric persistent launch.  Each job's output (keys, values, nnz) is
+ * exactly what gsparc_sptc returns for that job alone.  Jobs are grouped so
+ * that every group's prefixed keys fit 64 bits.  A job that fails (bad
+ * argument, out-of-range index) fails alone: its status says why and its sink
+ * gets nothing; the call then returns the first failing job's status.
+ * max_chunk_nnz (0 = from the HBM budget) bounds the output held in HBM at
+ * once, across the jobs of a group. */
+gsparc_status gsparc_sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz,
+                                gsparc_stats *stats, void *stream);
 
 /* ---- host helpers (no GPU needed) ---------------------------------------- */
 /* Parse a .tns file: 1-based text COO, one nonzero per line, order = tokens of

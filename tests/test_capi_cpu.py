@@ -30,6 +30,30 @@ def test_library_exports_every_declared_symbol():
     assert set(gb.EXPORTS) <= set(decl)
 
 
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Sizes and field offsets of the Python binding's structs equal the C ones."""
+    from gsparc_b200 import api
+    structs = {"gsparc_coo": api._Coo, "gsparc_sink": api._Sink, "gsparc_stats": api.Stats,
+               "gsparc_job": api._Job, "gsparc_digest": api.Digest}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "gsparc_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "abi.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.split("\n") if l)
+    for cname, py in structs.items():
+        import ctypes
+        assert int(out[cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(out[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"
+
+
 def test_version_and_status_strings():
     assert "sm_100a" in gb.version()
     assert gb.lib().gsparc_status_string(2) == b"out of memory"
