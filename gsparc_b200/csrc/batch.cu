@@ -120,9 +120,11 @@ __global__ void k_blin(const BLin *__restrict__ tab, const uint64_t *__restrict_
 }
 
 // Y: run boundaries of (job, contract key) and the prefixed free index.
+// A job whose Y repeats a coordinate gets ydup[job] set: its runs may hold a
+// free index twice, so none of its rows is streamed.
 __global__ void k_by_split(const uint64_t *__restrict__ ykeys, uint64_t ny, int kby,
                            const BPrep *__restrict__ jobs, uint8_t *__restrict__ run_flag,
-                           uint64_t *__restrict__ yfk) {
+                           uint64_t *__restrict__ yfk, unsigned int *__restrict__ ydup) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t km = low_mask(kby);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ny; i += stride) {
@@ -135,6 +137,7 @@ __global__ void k_by_split(const uint64_t *__restrict__ ykeys, uint64_t ny, int 
         if (i > 0) {
             const uint64_t pk = ykeys[i - 1];
             flag = (shr(pk, kby) != j) || (shr(pk & km, nfb) != c);
+            if (pk == key) atomicOr(&ydup[j], 1u);
         }
         run_flag[i] = flag;
         yfk[i] = shl(j, kby) | (loc & low_mask(nfb));
@@ -275,12 +278,13 @@ __global__ void k_brows(const uint64_t *__restrict__ xkeys, int kbx, const BPrep
     }
 }
 
-// Row classes: single-run rows stream (their output count is their product
-// count), other rows with more than the job's light limit of products are
+// Row classes: single-run rows of jobs without repeated Y coordinates stream
+// (their output count is their product count), other rows with more than the job's light limit of products are
 // heavy, the rest with products are light.  Rows outside [range[0],
 // range[1]) (a shard) get no class and no output.
 __global__ void k_bclass(const uint64_t *__restrict__ row_prod, const uint32_t *__restrict__ row_runs,
                          const uint16_t *__restrict__ row_job, const BPrep *__restrict__ jobs,
+                         const unsigned int *__restrict__ ydup,
                          const uint64_t *__restrict__ nrows_dev, const uint64_t *__restrict__ range, uint64_t nx,
                          uint8_t *__restrict__ heavy, uint8_t *__restrict__ lnz, uint8_t *__restrict__ sflag,
                          uint8_t *__restrict__ brk, uint64_t *__restrict__ lp, uint32_t *__restrict__ row_nnz) {
@@ -292,8 +296,9 @@ __global__ void k_bclass(const uint64_t *__restrict__ row_prod, const uint32_t *
         uint64_t p = 0;
         if (r < nr && r >= r0 && r < r1) {
             p = row_prod[r];
-            st = row_runs[r] == 1;
-            h = !st && p > jobs[row_job[r]].light_max;
+            const uint16_t j = row_job[r];
+            st = row_runs[r] == 1 && !ydup[j];
+            h = !st && p > jobs[j].light_max;
             l = !st && !h && p > 0;
             if (st) row_nnz[r] = (uint32_t)p;
         }
@@ -302,6 +307,37 @@ __global__ void k_bclass(const uint64_t *__restrict__ row_prod, const uint32_t *
         sflag[r] = st;
         brk[r] = h | st;
         lp[r] = l ? p : 0;
+    }
+}
+
+// Row range of one shard of a single job: shard s starts at the first row
+// whose product midpoint reaches s/n of the job's products, i.e. the first r
+// with n * (P[r] + P[r+1]) >= 2 * s * P[nrows] (P = row product prefix), the
+// exact-integer form of the host planner gs::plan_shards.
+// range = {first row, end row, products of the shard}.
+__device__ uint64_t shard_bound(const uint64_t *P, uint64_t nr, int s, int n) {
+    if (s <= 0) return 0;
+    if (s >= n) return nr;
+    const unsigned __int128 target = (unsigned __int128)2 * (unsigned)s * P[nr];
+    uint64_t lo = 0, hi = nr;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if ((unsigned __int128)(unsigned)n * ((unsigned __int128)P[mid] + P[mid + 1]) >= target)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return lo;
+}
+
+__global__ void k_shard_range(const uint64_t *__restrict__ P, const uint64_t *__restrict__ nrows_dev, int shard,
+                              int nshards, uint64_t *__restrict__ range) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint64_t nr = *nrows_dev;
+        const uint64_t a = shard_bound(P, nr, shard, nshards), b = shard_bound(P, nr, shard + 1, nshards);
+        range[0] = a;
+        range[1] = b;
+        range[2] = P[b] - P[a];
     }
 }
 
@@ -584,8 +620,8 @@ void deliver_slice(gsparc_sink &sink, const uint64_t *dk, const float *dv, uint6
     }
 }
 
-void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, Times &tm,
-               gsparc_stats &bst, cudaStream_t s) {
+void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, int shard, int nshards,
+               Times &tm, gsparc_stats &bst, cudaStream_t s) {
     Arena &A = ctx->arena;
     const int g = (int)G.size();
     const int jb = ceil_log2((uint64_t)g);
@@ -622,9 +658,9 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, T
     DBuf<BPrep> d_bp(A, g, s);
     DBuf<BatchJob> d_acc(A, g, s);
     DBuf<uint64_t> d_xoffs(A, g + 1, s), d_yoffs(A, g + 1, s);
-    DBuf<unsigned int> d_jerr(A, g, s);
+    DBuf<unsigned int> d_jerr(A, g, s), d_ydup(A, g, s);
     // 0 ncols, 1 nruns, 2 nrows, 3 heavy rows, 4 light rows, 5 light units, 6 largest unit output,
-    // 7 stream rows, 8 heavy + stream rows
+    // 7 stream rows, 8 heavy + stream rows, 9..11 shard row range and products
     DBuf<uint64_t> cnts(A, 16, s);
     h2d(d_lx.get(), lx.data(), g, s);
     h2d(d_ly.get(), ly.data(), g, s);
@@ -632,6 +668,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, T
     h2d(d_xoffs.get(), xoffs.data(), g + 1, s);
     h2d(d_yoffs.get(), yoffs.data(), g + 1, s);
     GS_CUDA(cudaMemsetAsync(d_jerr.get(), 0, 4 * g, s));
+    GS_CUDA(cudaMemsetAsync(d_ydup.get(), 0, 4 * g, s));
     GS_CUDA(cudaMemsetAsync(cnts.get(), 0, 128, s));
     GS_CUDA(cudaMemsetAsync(ctx->d_flag, 0, 4 * 4, s));
     bst.bytes_h2d += (sizeof(BLin) * 2 + sizeof(BPrep) + 16) * g;
@@ -672,7 +709,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, T
         DBuf<uint8_t> flag(A, nyb, s);
         DBuf<uint64_t> yf0(A, nyb, s), yf1(A, nyb, s);
         if (ny) {
-            k_by_split<<<grid_for(ny), kThreads, 0, s>>>(ykeys, ny, kby, d_bp, flag, yf0);
+            k_by_split<<<grid_for(ny), kThreads, 0, s>>>(ykeys, ny, kby, d_bp, flag, yf0, d_ydup);
             count_launch();
             GS_CUDA(cudaGetLastError());
         }
@@ -733,13 +770,23 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, T
         rflag.release();
         DBuf<uint8_t> heavy(A, nxb, s), lnz(A, nxb, s), sflag(A, nxb, s), brk(A, nxb, s);
         DBuf<uint64_t> lp(A, nxb, s);
+        GS_CUDA(cudaMemsetAsync(row_prod.get(), 0, 8 * nxb, s));
         k_brows<<<grid_for(nx + 1), kThreads, 0, s>>>(xkeys, kbx, d_bp, rsx, cnts.get() + 2, nx, xprefix, mpre,
                                                        row_start, row_xf, row_job, row_prod, row_runs, row_xi);
         count_launch();
         GS_CUDA(cudaGetLastError());
+        const uint64_t *range = nullptr;
+        if (nshards > 1) {
+            DBuf<uint64_t> rp(A, nx + 1, s);
+            prefix_sum(A, row_prod.get(), rp.get(), nx, s);
+            k_shard_range<<<1, 32, 0, s>>>(rp, cnts.get() + 2, shard, nshards, cnts.get() + 9);
+            count_launch();
+            GS_CUDA(cudaGetLastError());
+            range = cnts.get() + 9;
+        }
         if (nx) {
-            k_bclass<<<grid_for(nx), kThreads, 0, s>>>(row_prod, row_runs, row_job, d_bp, cnts.get() + 2, nullptr,
-                                                        nx, heavy, lnz, sflag, brk, lp, row_nnz);
+            k_bclass<<<grid_for(nx), kThreads, 0, s>>>(row_prod, row_runs, row_job, d_bp, d_ydup, cnts.get() + 2,
+                                                        range, nx, heavy, lnz, sflag, brk, lp, row_nnz);
             count_launch();
             GS_CUDA(cudaGetLastError());
         }
@@ -783,6 +830,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, T
     d2h(&ir, xprefix.get() + nx, 1, s);
     GS_CUDA(cudaStreamSynchronize(s));
     const uint64_t nrows = hc_cnt[2], nh = hc_cnt[3], nu = hc_cnt[5], nsr = hc_cnt[7];
+    if (nshards > 1) ir = hc_cnt[11];  // the shard's products
     bst.ir_nnz += ir;
     bst.rows += nrows;
     bst.heavy_rows += nh;
@@ -878,7 +926,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, T
     for (int j = 0; j < g; ++j) {
         gsparc_job &J = *G[j]->job;
         gsparc_stats &st = J.stats;
-        st.ir_nnz = jo[j + 1].ir_off - jo[j].ir_off;
+        st.ir_nnz = nshards > 1 ? ir : jo[j + 1].ir_off - jo[j].ir_off;
         st.nnz = jo[j + 1].out_off - jo[j].out_off;
         st.rows = jo[j + 1].row0 - jo[j].row0;
         st.heavy_rows = jo[j + 1].heavy0 - jo[j].heavy0;
@@ -1046,9 +1094,11 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, T
 }  // namespace
 
 void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st_out,
-                cudaStream_t s) {
+                cudaStream_t s, int shard, int nshards) {
     GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
     GS_REQUIRE(njobs >= 0 && (njobs == 0 || jobs), GSPARC_EINVAL, "bad job array");
+    GS_REQUIRE(nshards >= 1 && shard >= 0 && shard < nshards, GSPARC_EINVAL, "bad shard");
+    GS_REQUIRE(nshards == 1 || njobs == 1, GSPARC_EINVAL, "row shards apply to a single contraction");
     gsparc_stats bst;
     std::memset(&bst, 0, sizeof(bst));
     const uint64_t launches0 = launch_count();
@@ -1131,7 +1181,7 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
     Times tm;
     for (auto &G : groups) {
         try {
-            run_group(ctx, G, max_chunk_nnz, tm, bst, s);
+            run_group(ctx, G, max_chunk_nnz, shard, nshards, tm, bst, s);
         } catch (const Error &e) {
             // the group's jobs fail together; later groups still run
             for (Job *q : G)
@@ -1163,9 +1213,11 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
     }
     if (st_out) *st_out = bst;
     for (int i = 0; i < njobs; ++i)
-        if (jobs[i].status != GSPARC_OK)
+        if (jobs[i].status != GSPARC_OK) {
+            if (njobs == 1) fail(jobs[i].status, last_error());
             fail(jobs[i].status, std::string("job ") + std::to_string(i) + " failed (" +
                                      gsparc_status_string(jobs[i].status) + "); last message: " + last_error());
+        }
 }
 
 }  // namespace gs

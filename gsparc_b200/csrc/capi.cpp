@@ -191,7 +191,36 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
     return guard([&] {
         GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
         DeviceScope ds(ctx->device);
-        gs::sptc(ctx, X, Y, ncmodes, cx, cy, accum, shard, nshards, sink, stats, (cudaStream_t)stream);
+        // one contraction = a batch of one job
+        gsparc_job job;
+        std::memset(&job, 0, sizeof(job));
+        job.x = X;
+        job.y = Y;
+        job.ncmodes = ncmodes;
+        job.cx = cx;
+        job.cy = cy;
+        job.accum = accum;
+        if (sink) job.sink = *sink;
+        gsparc_stats bst;
+        std::memset(&bst, 0, sizeof(bst));
+        try {
+            gs::sptc_batch(ctx, &job, 1, sink ? sink->max_chunk_nnz : 0, &bst, (cudaStream_t)stream, shard,
+                           nshards);
+        } catch (const gs::Error &e) {
+            // the job's own status is the precise one
+            throw gs::Error{job.status != GSPARC_OK ? job.status : e.st, e.msg};
+        }
+        if (stats) {
+            gsparc_stats st = job.stats;
+            st.chunks = bst.chunks;
+            st.bytes_h2d = bst.bytes_h2d;
+            st.bytes_d2h = bst.bytes_d2h;
+            st.kernel_launches = bst.kernel_launches;
+            st.t_numeric_kernel_ms = bst.t_numeric_kernel_ms;
+            st.heavy_windows = bst.heavy_windows;
+            st.stream_rows = bst.stream_rows;
+            *stats = st;
+        }
     });
 }
 

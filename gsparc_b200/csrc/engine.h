@@ -7,13 +7,10 @@
 
 namespace gs {
 
-void sptc(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int nc, const int *cx,
-          const int *cy, int accum, int shard, int nshards, const gsparc_sink *sink,
-          gsparc_stats *st, cudaStream_t s);
-
-// Many contractions as one (batch.cu).
+// Many contractions as one (batch.cu).  A single contraction is a batch of one;
+// shard/nshards restrict a single job to one row shard (multi-GPU runs).
 void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st,
-                cudaStream_t s);
+                cudaStream_t s, int shard = 0, int nshards = 1);
 
 void plan_shards(const uint64_t *row_prod, uint64_t nrows, int nshards, uint64_t *bounds);
 

@@ -1,9 +1,9 @@
 // stream.cu -- output rows fed by a single matched Y run.
 //
 // When only one X nonzero of an output row matches, the row's products are
-// that nonzero times one Y run.  Y has unique coordinates, so the run's free
-// indices are distinct and already ascending: the row's output is the run
-// itself, one product per output, in order.  Its symbolic count is the run
+// that nonzero times one Y run.  When Y repeats no coordinate (the planner
+// checks), the run's free indices are distinct and already ascending: the
+// row's output is the run itself, one product per output, in order.  Its symbolic count is the run
 // length, and the numeric pass is a copy with a multiply: no sort, no
 // accumulator.  The value x*y rounded once is exactly what the compensated
 // accumulators return for a single product (0 + p is exact and p + fma error
