@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work per baseline sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-stream (batched / served) lines")
+    ap.add_argument("--mixed-count", type=int, default=256, help="instances of the mixed stream")
     return ap.parse_args()
 
 
@@ -212,6 +214,131 @@ class CpuBaseline:
                              if self.kind == "reference" else "CPU oracle (ESC, FP64), wall time")}
 
 
+def mixed_stream(args, device, sp, stream):
+    """The mixed stream of independent contractions (orders 3-4, modes
+    log-uniform 64..100k, nnz log-uniform 1e3..1e6, 1-2 contract modes,
+    Zipf s in [1.0,1.4], U[-1,1), seed 3), run three ways on the same
+    resident operands: plain (one gsparc_sptc per contraction, in order),
+    batched (one gsparc_sptc_batch) and served (Poisson arrivals at a mean
+    2000 requests/s into a gsparc_serve_* server; the plain form answers the
+    same arrivals one at a time)."""
+    import torch
+    import gsparc_b200 as gb
+    from gsparc_b200 import synth
+    inst = synth.batched_instances(args.mixed_count, seed=3, max_nnz=1_000_000)
+    ctx = gb.Context(device)
+    ops = [(ctx.upload(X, stream=sp), ctx.upload(Y, stream=sp)) for X, Y, _, _ in inst]
+    jobs = [(dx, dy, cx, cy) for (dx, dy), (_, _, cx, cy) in zip(ops, inst)]
+    nnz = sum(X.nnz + Y.nnz for X, Y, _, _ in inst)
+
+    def plain_once():
+        return sum(gb.sptc(ctx, dx, dy, cx, cy, 0, sink="discard", stream=sp).ir_nnz for dx, dy, cx, cy in jobs)
+
+    def batched_once():
+        res, bst = gb.sptc_batch(ctx, jobs, sink="discard", stream=sp)
+        return bst
+
+    # warm-up of both forms
+    plain_once()
+    batched_once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ir = plain_once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    e0.record(stream)
+    bst = batched_once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = e0.elapsed_time(e1)
+    assert bst["ir_nnz"] == ir
+
+    for dx, dy in ops:
+        dx.free()
+        dy.free()
+    ctx.close()  # the server gets the device's memory to itself
+
+    # served: the same contractions arriving as a Poisson stream
+    rng = np.random.default_rng(17)
+    arrive = np.cumsum(rng.exponential(1.0 / 2000.0, size=len(jobs)))
+    free_b, _ = torch.cuda.mem_get_info()
+    budget = min(150 << 30, int(free_b * 0.9))
+
+    def served_run(lanes):
+        srv = gb.Server(device, hbm_budget=budget, lanes=lanes)
+        sops = [(srv.upload(X), srv.upload(Y)) for X, Y, _, _ in inst]
+        # warm-up: the whole stream once, unpaced (as the other forms get one pass)
+        for t in [srv.submit(sx, sy, cx, cy, sink="discard") for (sx, sy), (_, _, cx, cy) in zip(sops, inst)]:
+            srv.wait(t)
+        srv.reset_stats()
+        tickets = [None] * len(jobs)
+
+        def client():
+            t0 = time.perf_counter()
+            for i, ((sx, sy), (_, _, cx, cy)) in enumerate(zip(sops, inst)):
+                d = t0 + arrive[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets[i] = srv.submit(sx, sy, cx, cy, sink="discard")
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        for t in tickets:
+            srv.wait(t)
+        st = srv.stats()
+        srv.close()
+        return st
+    sst = served_run(2)  # the server's default: two lanes
+    sst1 = served_run(1)
+
+    # plain form on the same arrivals: one contraction at a time, in order
+    ctx = gb.Context(device)
+    ops = [(ctx.upload(X, stream=sp), ctx.upload(Y, stream=sp)) for X, Y, _, _ in inst]
+    jobs = [(dx, dy, cx, cy) for (dx, dy), (_, _, cx, cy) in zip(ops, inst)]
+    plain_once()
+    torch.cuda.synchronize()
+    lat = []
+    t0 = time.perf_counter()
+    for i, (dx, dy, cx, cy) in enumerate(jobs):
+        d = t0 + arrive[i] - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        gb.sptc(ctx, dx, dy, cx, cy, 0, sink="discard", stream=sp)
+        lat.append((time.perf_counter() - t0 - arrive[i]) * 1e3)
+    plain_wall = time.perf_counter() - t0
+    lat = np.sort(np.asarray(lat))
+
+    def pct(v, p):
+        return float(v[max(1, int(math.ceil(p / 100.0 * len(v)))) - 1])
+    for dx, dy in ops:
+        dx.free()
+        dy.free()
+    ctx.close()
+    desc = (f"{len(jobs)} independent contractions, {nnz} operand nonzeros, {ir:.4e} matched products "
+            "(orders 3-4, modes log-uniform 64..100k, nnz log-uniform 1e3..1e6, 1-2 contract modes, "
+            "Zipf s 1.0-1.4, U[-1,1), seed 3)")
+    batched = {"workload": desc, "unit": UNIT,
+               "plain_value": ir / (plain_ms / 1e3), "plain_ms": plain_ms,
+               "batched_value": ir / (batched_ms / 1e3), "batched_ms": batched_ms,
+               "batched_over_plain": plain_ms / batched_ms, "groups_launches": bst["kernel_launches"],
+               "timing": "CUDA events on the launching stream, each form after one warm-up pass"}
+    served = {"workload": desc + f"; Poisson arrivals, mean 2000/s, seed 17; HBM budget {budget / 2**30:.0f} GiB",
+              "unit": UNIT, "value": sst["products_per_s"], "p50_ms": sst["p50_ms"], "p99_ms": sst["p99_ms"],
+              "mean_ms": sst["mean_ms"], "wall_ms": sst["wall_ms"], "batches": sst["batches"],
+              "max_batch": sst["max_batch"], "max_in_flight": sst["max_in_flight"],
+              "plain_value": ir / plain_wall, "plain_p50_ms": pct(lat, 50), "plain_p99_ms": pct(lat, 99),
+              "plain_wall_ms": plain_wall * 1e3, "served_over_plain": sst["products_per_s"] / (ir / plain_wall),
+              "lanes": 2,
+              "one_lane": {"value": sst1["products_per_s"], "p50_ms": sst1["p50_ms"], "p99_ms": sst1["p99_ms"],
+                           "wall_ms": sst1["wall_ms"], "batches": sst1["batches"],
+                           "served_over_plain": sst1["products_per_s"] / (ir / plain_wall)},
+              "timing": "host clock: latency = submission to result delivered; the plain form runs "
+                        "each request when it has arrived and the previous one finished"}
+    return batched, served
+
+
 # --------------------------------------------------------------------------- arms
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -367,6 +494,11 @@ def ours_arm(args, world, rank, local, dist):
                "ms_per_step": ems / ks, "steps": ks,
                "sink": f"pinned host ring of {ring} nonzeros, every output chunk copied"}
 
+    ctx.close()  # returns the large workload's memory before the mixed stream
+    batched = served = None
+    if world == 1 and not args.no_mixed:
+        batched, served = mixed_stream(args, local, sp, stream)
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         base = CpuBaseline(X, target_seconds=args.cpu_seconds)
@@ -388,12 +520,13 @@ def ours_arm(args, world, rank, local, dist):
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "batched": batched,
+            "served": served,
             "heavy_windows": s0["heavy_windows"], "heavy_rows": s0["heavy_rows"], "rows": s0["rows"],
             "stage_ms": {k: s0[k] for k in ("t_linearize_ms", "t_sort_ms", "t_match_ms", "t_plan_ms",
                                              "t_contract_ms", "t_total_ms")},
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
 
 
 def main():

@@ -84,6 +84,9 @@ EXPORTS = [
     "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
     "gsparc_free_host", "gsparc_layout", "gsparc_plan_shards", "gsparc_linearize",
     "gsparc_sort_pairs", "gsparc_index_match", "gsparc_digest_chunk", "gsparc_sptc_batch",
+    "gsparc_serve_create", "gsparc_serve_destroy", "gsparc_serve_upload", "gsparc_serve_release",
+    "gsparc_serve_submit", "gsparc_serve_poll", "gsparc_serve_wait", "gsparc_serve_stats",
+    "gsparc_serve_reset_stats",
 ]
 
 
@@ -91,6 +94,24 @@ class _Job(ctypes.Structure):
     _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("ncmodes", ctypes.c_int),
                 ("cx", ctypes.c_void_p), ("cy", ctypes.c_void_p), ("accum", ctypes.c_int),
                 ("sink", _Sink), ("stats", Stats), ("status", ctypes.c_int)]
+
+
+class _ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("lanes", ctypes.c_int),
+                ("max_batch_jobs", ctypes.c_int), ("max_batch_nnz", ctypes.c_uint64),
+                ("fifo", ctypes.c_int), ("age_ms", ctypes.c_double), ("max_chunk_nnz", ctypes.c_uint64)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("batches", ctypes.c_uint64), ("max_batch", ctypes.c_uint64), ("ir_nnz", ctypes.c_uint64),
+                ("nnz", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
+                ("products_per_s", ctypes.c_double), ("resident_bytes", ctypes.c_uint64),
+                ("peak_reserved_bytes", ctypes.c_uint64), ("max_in_flight", ctypes.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Digest(ctypes.Structure):
@@ -134,6 +155,15 @@ def lib():
     L.gsparc_index_match.argtypes = [P, U64, P, I, U64, P, I, P, P, P, P, P]
     L.gsparc_digest_chunk.argtypes = [P, P, U64, ctypes.POINTER(Digest), P]
     L.gsparc_sptc_batch.argtypes = [P, P, I, U64, ctypes.POINTER(Stats), P]
+    L.gsparc_serve_create.argtypes = [I, ctypes.POINTER(_ServerOpts), ctypes.POINTER(P)]
+    L.gsparc_serve_destroy.argtypes = [P]
+    L.gsparc_serve_upload.argtypes = [P, ctypes.POINTER(_Coo), ctypes.POINTER(P)]
+    L.gsparc_serve_release.argtypes = [P, P]
+    L.gsparc_serve_submit.argtypes = [P, ctypes.POINTER(_Job), ctypes.POINTER(U64)]
+    L.gsparc_serve_poll.argtypes = [P, U64, ctypes.POINTER(I), ctypes.POINTER(_Job)]
+    L.gsparc_serve_wait.argtypes = [P, U64, ctypes.c_double, ctypes.POINTER(_Job)]
+    L.gsparc_serve_stats.argtypes = [P, ctypes.POINTER(ServeStats)]
+    L.gsparc_serve_reset_stats.argtypes = [P]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype if name in (
             "gsparc_version", "gsparc_status_string", "gsparc_last_error") else (
@@ -469,6 +499,146 @@ def sptc_batch(ctx: Context, jobs, sink: str = "host", max_chunk_nnz: int = 0, s
     bd = st.as_dict()
     bd["status"] = int(rc)
     return results, bd
+
+
+class ServerTensor:
+    """An operand resident in a :class:`Server`'s HBM budget."""
+
+    def __init__(self, srv: "Server", t: CooTensor):
+        self.srv = srv
+        self._h = ctypes.c_void_p()
+        self.dims = [int(d) for d in t.dims]
+        self.order = len(self.dims)
+        dims = np.asarray(self.dims, np.uint64)
+        idx = np.ascontiguousarray(t.idx, np.uint64)
+        val = np.ascontiguousarray(t.val, np.float32)
+        self.nnz = int(val.shape[0])
+        arr = (ctypes.c_void_p * max(self.order, 1))(*[idx[m].ctypes.data for m in range(self.order)])
+        coo = _Coo(self.order, dims.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), self.nnz, arr,
+                   val.ctypes.data, 0)
+        _check(lib().gsparc_serve_upload(srv.handle, ctypes.byref(coo), ctypes.byref(self._h)), "serve_upload")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def release(self):
+        if self._h and self.srv.handle:
+            _check(lib().gsparc_serve_release(self.srv.handle, self._h), "serve_release")
+        self._h = ctypes.c_void_p()
+
+
+class Server:
+    """Request loop with continuous batching (gsparc_serve_*).
+
+    ``submit`` queues a contraction of resident operands and returns a ticket;
+    ``wait`` returns its :class:`SpTCResult`.  Free lanes take waiting
+    requests (shortest first, or in arrival order once they waited longer
+    than ``age_ms``; ``fifo`` keeps arrival order), as many as the HBM budget
+    admits, and run them as one batch; lanes run concurrently on their own
+    streams.
+    """
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, lanes: int = 0, max_batch_jobs: int = 0,
+                 max_batch_nnz: int = 0, fifo: bool = False, age_ms: float = 0.0, max_chunk_nnz: int = 0):
+        o = _ServerOpts(hbm_budget, lanes, max_batch_jobs, max_batch_nnz, int(fifo), age_ms, max_chunk_nnz)
+        self._h = ctypes.c_void_p()
+        _check(lib().gsparc_serve_create(device, ctypes.byref(o), ctypes.byref(self._h)), "serve_create")
+        self._pending = {}
+
+    @property
+    def handle(self):
+        return self._h
+
+    def upload(self, t: CooTensor) -> ServerTensor:
+        return ServerTensor(self, t)
+
+    def submit(self, X: ServerTensor, Y: ServerTensor, cx: Sequence[int], cy: Sequence[int],
+               dense_accumulator: int = ACCUM_AUTO, sink: str = "host", staging: int = 1 << 20) -> int:
+        """Queue Z = X x_{cx,cy} Y; sink "host" (Z returned by wait) or "discard"."""
+        if len(cx) != len(cy):
+            raise ValueError("cx and cy must have the same length")
+        c1 = np.asarray(cx, np.int32)
+        c2 = np.asarray(cy, np.int32)
+        J = _Job()
+        J.x, J.y = X.handle, Y.handle
+        J.ncmodes = len(c1)
+        J.cx, J.cy = c1.ctypes.data, c2.ctypes.data
+        J.accum = int(dense_accumulator)
+        keep = [c1, c2]
+        parts = []
+        if sink == "host":
+            hk = np.zeros(staging, np.uint64)
+            hv = np.zeros(staging, np.float32)
+
+            def _cbh(user, k, v, m, first, on_dev):
+                kk = np.ctypeslib.as_array(ctypes.cast(k, ctypes.POINTER(ctypes.c_uint64)), shape=(m,)).copy()
+                vv = np.ctypeslib.as_array(ctypes.cast(v, ctypes.POINTER(ctypes.c_float)), shape=(m,)).copy()
+                parts.append((first, kk, vv))
+                return 0
+            cb = CHUNK_FN(_cbh)
+            keep += [hk, hv, cb]
+            J.sink.kind = SINK_HOST
+            J.sink.host_keys = hk.ctypes.data
+            J.sink.host_vals = hv.ctypes.data
+            J.sink.host_capacity = staging
+            J.sink.on_chunk = cb
+        elif sink == "discard":
+            J.sink.kind = SINK_DISCARD
+        else:
+            raise ValueError(f"unknown sink {sink!r}")
+        t = ctypes.c_uint64()
+        _check(lib().gsparc_serve_submit(self._h, ctypes.byref(J), ctypes.byref(t)), "serve_submit")
+        self._pending[t.value] = (keep, parts, sink)
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        d = ctypes.c_int()
+        _check(lib().gsparc_serve_poll(self._h, ticket, ctypes.byref(d), None), "serve_poll")
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0, raise_on_error: bool = True) -> SpTCResult:
+        J = _Job()
+        rc = lib().gsparc_serve_wait(self._h, ticket, timeout_ms, ctypes.byref(J))
+        if rc == 5:  # ETIMEOUT: still pending
+            _check(rc, "serve_wait")
+        keep, parts, sink = self._pending.pop(ticket, (None, [], "discard"))
+        if rc != 0 and raise_on_error:
+            _check(rc, "serve_wait")
+        d = J.stats.as_dict()
+        d["status"] = int(J.status) if rc == 0 else int(rc)
+        keys = vals = None
+        if rc == 0 and sink == "host":
+            ps = sorted(parts, key=lambda p: p[0])
+            keys = np.concatenate([p[1] for p in ps]) if ps else np.zeros(0, np.uint64)
+            vals = np.concatenate([p[2] for p in ps]) if ps else np.zeros(0, np.float32)
+        return SpTCResult(int(J.stats.nnz), int(J.stats.ir_nnz), keys, vals, d)
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        _check(lib().gsparc_serve_stats(self._h, ctypes.byref(st)), "serve_stats")
+        return st.as_dict()
+
+    def reset_stats(self) -> None:
+        _check(lib().gsparc_serve_reset_stats(self._h), "serve_reset_stats")
+
+    def close(self) -> None:
+        if self._h:
+            _check(lib().gsparc_serve_destroy(self._h), "serve_destroy")
+            self._h = ctypes.c_void_p()
+            self._pending.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def SpTC(X: CooTensor, Y: CooTensor, cx: Sequence[int], cy: Sequence[int],

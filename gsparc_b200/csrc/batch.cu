@@ -483,17 +483,17 @@ __global__ void k_merge_starts(UnitLists u, const uint64_t *__restrict__ row_off
     }
 }
 
-// Chunk k starts at the first unit whose output starts at or after k*C.
-// info[5k..5k+4] = first row, first output, first light unit, first heavy
-// row (row-ordered index), first stream row of chunk k; entry K closes the
-// last chunk.
+// Chunk k starts at the first unit whose output starts at or after
+// target[k] (target[0] = 0, increasing).  info[5k..5k+4] = first row, first
+// output, first light unit, first heavy row (row-ordered index), first stream
+// row of chunk k; entry K closes the last chunk.
 constexpr int kChunkInfo = 5;
 __global__ void k_chunk_bounds(const uint32_t *__restrict__ urow, const uint64_t *__restrict__ uoff, uint64_t M,
-                               uint64_t C, uint64_t K, UnitLists u, uint64_t nrows, uint64_t ntot,
-                               uint64_t *__restrict__ info) {
+                               const uint64_t *__restrict__ target, uint64_t K, UnitLists u, uint64_t nrows,
+                               uint64_t ntot, uint64_t *__restrict__ info) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= K; k += stride) {
-        const uint64_t b = k == 0 ? 0 : (k == K ? M : lower_bound_dev<uint64_t>(uoff, 0, M, k * C));
+        const uint64_t b = k == 0 ? 0 : (k == K ? M : lower_bound_dev<uint64_t>(uoff, 0, M, target[k]));
         const uint32_t row = (uint32_t)(b < M ? urow[b] : nrows);
         uint64_t *o = info + kChunkInfo * k;
         o[0] = row;
@@ -578,8 +578,14 @@ struct Job {
     gsparc_job *job;
     Layout LX, LY;
     uint64_t light_max;
-    int width;  // widest operand key
+    int width;          // widest operand key
+    bool done = false;  // reported through the completion callback
 };
+
+// First product count after which a job boundary closes a chunk when jobs
+// complete one by one (about a millisecond of accumulation); each further cut
+// waits for twice as many products, so a batch has O(log) extra chunks.
+constexpr uint64_t kFirstCutProducts = 1ull << 26;
 
 struct Times {
     double lin = 0, sort = 0, match = 0, plan = 0, contract = 0, out = 0, total = 0, numeric = 0;
@@ -621,7 +627,7 @@ void deliver_slice(gsparc_sink &sink, const uint64_t *dk, const float *dv, uint6
 }
 
 void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, int shard, int nshards,
-               Times &tm, gsparc_stats &bst, cudaStream_t s) {
+               Times &tm, gsparc_stats &bst, cudaStream_t s, const JobDoneFn *done_fn) {
     Arena &A = ctx->arena;
     const int g = (int)G.size();
     const int jb = ceil_log2((uint64_t)g);
@@ -954,22 +960,44 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     std::vector<Chunk> chunks;
     DBuf<uint32_t> Hc;  // heavy rows grouped by chunk, largest first inside a chunk
     const uint32_t *Hchunk = Hs;
-    if (ntot <= cap) {
+    // Jobs that complete one by one get chunk cuts at job boundaries after
+    // kFirstCutProducts, 2x that, 4x that, ... products.
+    const bool progressive = done_fn && g > 1 && ntot > 0;
+    if (ntot <= cap && !progressive) {
         if (ntot || nu || nh || nsr) chunks.push_back({0, nu, 0, nh, 0, nsr, 0, ntot});
     } else {
         uint64_t C = std::max(cap > max_unit ? cap - max_unit : 1, std::max<uint64_t>(max_unit, 1));
-        C = std::max<uint64_t>(C, (ntot + (1ull << 20) - 1) >> 20);  // at most 2^20 chunks
+        C = std::max<uint64_t>(C, (ntot + (1ull << 20) - 1) >> 20);  // at most 2^20 uniform chunks
         GS_REQUIRE(2 * 12 * (C + max_unit) <= A.available(), GSPARC_ENOMEM,
                    "one output row does not fit the HBM budget");
-        const uint64_t K = (ntot + C - 1) / C;
+        std::vector<uint64_t> target{0};
+        if (!progressive) {
+            for (uint64_t t = C; t < ntot; t += C) target.push_back(t);
+        } else {
+            uint64_t acc = 0, thr = kFirstCutProducts;
+            for (int j = 0; j < g; ++j) {
+                const uint64_t end = jo[j + 1].out_off;
+                while (end - target.back() > C) target.push_back(target.back() + C);
+                acc += jo[j + 1].ir_off - jo[j].ir_off;
+                if (acc >= thr && j + 1 < g && end > target.back() && end < ntot) {
+                    target.push_back(end);
+                    acc = 0;
+                    thr *= 2;
+                }
+            }
+        }
+        target.push_back(ntot);
+        const uint64_t K = target.size() - 1;
         const uint64_t M = nu + nh + nsr;
         DBuf<uint32_t> urow(A, M, s);
         DBuf<uint64_t> uoff(A, M, s);
         k_merge_starts<<<grid_for(M), kThreads, 0, s>>>(ul, row_off, urow, uoff);
         count_launch();
         GS_CUDA(cudaGetLastError());
+        DBuf<uint64_t> d_target(A, K + 1, s);
+        h2d(d_target.get(), target.data(), K + 1, s);
         DBuf<uint64_t> cinfo(A, kChunkInfo * (K + 1), s);
-        k_chunk_bounds<<<grid_for(K + 1), kThreads, 0, s>>>(urow, uoff, M, C, K, ul, nrows, ntot, cinfo);
+        k_chunk_bounds<<<grid_for(K + 1), kThreads, 0, s>>>(urow, uoff, M, d_target, K, ul, nrows, ntot, cinfo);
         count_launch();
         GS_CUDA(cudaGetLastError());
         std::vector<uint64_t> ci(kChunkInfo * (K + 1));
@@ -1015,6 +1043,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     double t_out = 0;
     std::vector<uint64_t> job_first(g + 1);
     for (int j = 0; j <= g; ++j) job_first[j] = jo[j].out_off;
+    int next_done = 0;  // jobs before it were reported complete
 
     auto enqueue = [&](size_t ci) {
         const Chunk &c = chunks[ci];
@@ -1056,6 +1085,22 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
                           a0 - job_first[j], job_nnz[j], s2, J.stats, bst.bytes_d2h);
         }
         t_out += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        // jobs whose whole output is now delivered are complete (unless a
+        // device-side check of the chunk failed)
+        if (done_fn && next_done < g && job_first[next_done + 1] <= c1) {
+            unsigned int e = 0;
+            d2h(&e, ctx->d_flag, 1, s2);
+            GS_CUDA(cudaStreamSynchronize(s2));
+            GS_REQUIRE(!(e & 6u), GSPARC_EINTERNAL, "numeric pass failed a device-side check");
+        }
+        if (done_fn)
+            for (; next_done < g && job_first[next_done + 1] <= c1; ++next_done) {
+                Job *q = G[next_done];
+                if (!q->done && q->job->status == GSPARC_OK) {
+                    q->done = true;
+                    (*done_fn)(q->job);
+                }
+            }
     };
     try {
         for (size_t ci = 0; ci < chunks.size(); ++ci) {
@@ -1094,7 +1139,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
 }  // namespace
 
 void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st_out,
-                cudaStream_t s, int shard, int nshards) {
+                cudaStream_t s, int shard, int nshards, const JobDoneFn *done_fn) {
     GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
     GS_REQUIRE(njobs >= 0 && (njobs == 0 || jobs), GSPARC_EINVAL, "bad job array");
     GS_REQUIRE(nshards >= 1 && shard >= 0 && shard < nshards, GSPARC_EINVAL, "bad shard");
@@ -1178,14 +1223,27 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
         }
     }
 
+    // completion reports: at most one per job, early ones from run_group
+    std::vector<char> reported(njobs, 0);
+    JobDoneFn report;
+    const JobDoneFn *report_fn = nullptr;
+    if (done_fn) {
+        report = [&](gsparc_job *J) {
+            reported[J - jobs] = 1;
+            (*done_fn)(J);
+        };
+        report_fn = &report;
+    }
+
     Times tm;
     for (auto &G : groups) {
         try {
-            run_group(ctx, G, max_chunk_nnz, shard, nshards, tm, bst, s);
+            run_group(ctx, G, max_chunk_nnz, shard, nshards, tm, bst, s, report_fn);
         } catch (const Error &e) {
-            // the group's jobs fail together; later groups still run
+            // the group's jobs fail together (except those already complete);
+            // later groups still run
             for (Job *q : G)
-                if (q->job->status == GSPARC_OK) q->job->status = e.st;
+                if (!q->done && q->job->status == GSPARC_OK) q->job->status = e.st;
             set_last_error(e.msg);
             cudaStreamSynchronize(s);
         }
@@ -1212,6 +1270,9 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
         st.t_total_ms = tm.total;
     }
     if (st_out) *st_out = bst;
+    if (done_fn)
+        for (int i = 0; i < njobs; ++i)
+            if (!reported[i]) (*done_fn)(&jobs[i]);
     for (int i = 0; i < njobs; ++i)
         if (jobs[i].status != GSPARC_OK) {
             if (njobs == 1) fail(jobs[i].status, last_error());

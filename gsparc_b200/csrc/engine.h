@@ -3,14 +3,23 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
+
 #include "internal.h"
 
 namespace gs {
 
+// Called once per job as soon as the job's whole output was delivered to its
+// sink (or it failed); the job's status and counts are final by then.
+using JobDoneFn = std::function<void(gsparc_job *)>;
+
 // Many contractions as one (batch.cu).  A single contraction is a batch of one;
-// shard/nshards restrict a single job to one row shard (multi-GPU runs).
+// shard/nshards restrict a single job to one row shard (multi-GPU runs).  With
+// done_fn, jobs complete one by one: the numeric pass is cut into chunks at job
+// boundaries of geometrically growing product counts, so a job finishes
+// when the chunks holding its rows are delivered, not at the end of the batch.
 void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st,
-                cudaStream_t s, int shard = 0, int nshards = 1);
+                cudaStream_t s, int shard = 0, int nshards = 1, const JobDoneFn *done_fn = nullptr);
 
 void plan_shards(const uint64_t *row_prod, uint64_t nrows, int nshards, uint64_t *bounds);
 

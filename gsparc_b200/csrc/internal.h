@@ -67,6 +67,11 @@ public:
     Arena() = default;
     ~Arena();
     void init(int device, uint64_t budget);
+    // Draw from a pool owned elsewhere (several arenas on one pool, each with
+    // its own budget); the pool outlives the arena.
+    void init_shared(int device, cudaMemPool_t pool, uint64_t budget);
+    void set_budget(uint64_t budget) { budget_ = budget; }
+    void reset_peak() { peak_ = in_use_; }
     void *alloc(size_t bytes, cudaStream_t s);
     void free(void *p, cudaStream_t s);
     uint64_t in_use() const { return in_use_; }
@@ -74,10 +79,12 @@ public:
     uint64_t budget() const { return budget_; }
     uint64_t available() const { return budget_ > in_use_ ? budget_ - in_use_ : 0; }
     int device() const { return device_; }
+    cudaMemPool_t pool() const { return pool_; }
 
 private:
     int device_ = -1;
     cudaMemPool_t pool_ = nullptr;
+    bool owns_pool_ = false;
     uint64_t budget_ = 0, in_use_ = 0, peak_ = 0;
     std::unordered_map<void *, size_t> sizes_;
 };

@@ -59,7 +59,7 @@ Layout make_layout(int order, const uint64_t *dims, int nc, const int *cmodes) {
 }
 
 Arena::~Arena() {
-    if (pool_) {
+    if (pool_ && owns_pool_) {
         // Outstanding buffers belong to objects that are being torn down too.
         cudaMemPoolDestroy(pool_);
     }
@@ -75,8 +75,16 @@ void Arena::init(int device, uint64_t budget) {
     props.location.type = cudaMemLocationTypeDevice;
     props.location.id = device;
     GS_CUDA(cudaMemPoolCreate(&pool_, &props));
+    owns_pool_ = true;
     uint64_t thr = UINT64_MAX;
     GS_CUDA(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &thr));
+}
+
+void Arena::init_shared(int device, cudaMemPool_t pool, uint64_t budget) {
+    device_ = device;
+    budget_ = budget;
+    pool_ = pool;
+    owns_pool_ = false;
 }
 
 void *Arena::alloc(size_t bytes, cudaStream_t s) {

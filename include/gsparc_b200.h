@@ -188,6 +188,74 @@ typedef struct {
 gsparc_status gsparc_sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz,
                                 gsparc_stats *stats, void *stream);
 
+/* ---- serving: a request loop over resident operands ----------------------- */
+/* No counterpart in the reference, which runs one contraction per process
+ * (main.cu:22-437).  A server owns one device, an HBM budget shared by its
+ * resident operands and the working memory of the contractions in flight,
+ * and `lanes` worker threads, each with its own CUDA stream.  A free lane
+ * takes waiting requests, as many as the free budget and the batch limits
+ * admit, and runs them as one gsparc_sptc_batch; requests that arrive
+ * meanwhile wait for the next free lane, so batches of different lanes
+ * overlap on the device.  Small requests go first unless one has waited
+ * longer than age_ms (shortest first with ageing), so a small request is not
+ * queued behind a large one that arrived just before it.  A request whose
+ * output does not fit the HBM
+ * budget streams it in chunks like gsparc_sptc.  Submit, poll, wait, stats
+ * and upload may be called from any thread. */
+typedef struct gsparc_server gsparc_server;
+
+typedef struct {
+    uint64_t hbm_budget_bytes; /* resident operands + work in flight (0 = 90% of free HBM) */
+    int lanes;                 /* worker threads / streams (0 = 2)                          */
+    int max_batch_jobs;        /* requests per batch (0 = 256)                              */
+    uint64_t max_batch_nnz;    /* operand nonzeros per batch, X + Y (0 = 2^24); a request
+                                * larger than this runs in a batch of its own              */
+    int fifo;                  /* 1: admit in arrival order.  0: requests that waited
+                                * longer than age_ms first, in arrival order, then the
+                                * others smallest first (fewest operand nonzeros)          */
+    double age_ms;             /* 0 = 200 ms                                                */
+    uint64_t max_chunk_nnz;    /* output nonzeros per chunk (0 = 2^28): bounds the output
+                                * buffers a lane holds, larger outputs stream through     */
+} gsparc_server_opts;
+
+typedef struct {
+    uint64_t submitted, completed, failed;
+    uint64_t batches;          /* batches run                                               */
+    uint64_t max_batch;        /* most requests in one batch                                */
+    uint64_t ir_nnz, nnz;      /* matched products / output nonzeros of completed requests  */
+    double p50_ms, p99_ms;     /* latency: submission to result delivered                   */
+    double mean_ms, max_ms;
+    double wall_ms;            /* first submission to last completion                       */
+    double products_per_s;     /* ir_nnz / wall                                             */
+    uint64_t resident_bytes;   /* operands held by the server                               */
+    uint64_t peak_reserved_bytes; /* largest working memory admitted at once                */
+    uint64_t max_in_flight;    /* most batches running at once                              */
+} gsparc_server_stats;
+
+gsparc_status gsparc_serve_create(int device, const gsparc_server_opts *opts, gsparc_server **out);
+/* Waits for every submitted request, then stops the lanes and frees all
+ * resident operands. */
+gsparc_status gsparc_serve_destroy(gsparc_server *srv);
+/* Upload an operand that stays resident in the server's budget; requests name
+ * it by the returned handle.  Release frees it once no waiting or running
+ * request uses it. */
+gsparc_status gsparc_serve_upload(gsparc_server *srv, const gsparc_coo *coo, gsparc_tensor **out);
+gsparc_status gsparc_serve_release(gsparc_server *srv, gsparc_tensor *t);
+/* Queue one contraction.  The job is copied (cx/cy included); its sink, the
+ * sink's buffers and callback must stay valid until the request completes.
+ * The sink's callbacks run on a lane thread. */
+gsparc_status gsparc_serve_submit(gsparc_server *srv, const gsparc_job *job, uint64_t *ticket);
+/* done = 1 once the request completed; result (optional) then receives the
+ * job with its status and stats.  Poll does not block. */
+gsparc_status gsparc_serve_poll(gsparc_server *srv, uint64_t ticket, int *done, gsparc_job *result);
+/* Block until the request completes or timeout_ms passes (< 0: no limit;
+ * GSPARC_ETIMEOUT if it did not complete).  The ticket is retired after a
+ * completed wait. */
+gsparc_status gsparc_serve_wait(gsparc_server *srv, uint64_t ticket, double timeout_ms, gsparc_job *result);
+gsparc_status gsparc_serve_stats(gsparc_server *srv, gsparc_server_stats *out);
+/* Forget the latency samples and counters (after a warm-up). */
+gsparc_status gsparc_serve_reset_stats(gsparc_server *srv);
+
 /* ---- host helpers (no GPU needed) ---------------------------------------- */
 /* Parse a .tns file: 1-based text COO, one nonzero per line, order = tokens of
  * the first line minus one, dims[m] = largest index + 1.  Replaces
