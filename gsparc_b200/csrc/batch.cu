@@ -27,6 +27,7 @@
 
 #include "engine.h"
 #include "kernels.cuh"
+#include "wide.h"
 
 namespace gs {
 
@@ -576,6 +577,8 @@ inline int ceil_log2(uint64_t n) {
 
 struct Job {
     gsparc_job *job;
+    const gsparc_tensor *tx, *ty;   // the operands the engine runs on (relabeled when wide)
+    std::shared_ptr<WideMap> wide;  // set when the operand keys need more than 64 bits
     Layout LX, LY;
     uint64_t light_max;
     int width;          // widest operand key
@@ -653,10 +656,11 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     std::vector<BPrep> bp(g);
     for (int j = 0; j < g; ++j) {
         const gsparc_job &J = *G[j]->job;
-        xoffs[j + 1] = xoffs[j] + J.x->nnz;
-        yoffs[j + 1] = yoffs[j] + J.y->nnz;
-        lx[j] = {make_lin_params(G[j]->LX, J.x->dims, 0), J.x->d_idx, J.x->d_val, J.x->nnz};
-        ly[j] = {make_lin_params(G[j]->LY, J.y->dims, 1), J.y->d_idx, J.y->d_val, J.y->nnz};
+        const gsparc_tensor *tx = G[j]->tx, *ty = G[j]->ty;
+        xoffs[j + 1] = xoffs[j] + tx->nnz;
+        yoffs[j + 1] = yoffs[j] + ty->nnz;
+        lx[j] = {make_lin_params(G[j]->LX, tx->dims, 0), tx->d_idx, tx->d_val, tx->nnz};
+        ly[j] = {make_lin_params(G[j]->LY, ty->dims, 1), ty->d_idx, ty->d_val, ty->nnz};
         bp[j] = {G[j]->LX.ncbits, G[j]->LY.nfbits, G[j]->light_max};
     }
     const uint64_t nx = xoffs[g], ny = yoffs[g];
@@ -948,8 +952,10 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     // takes the units that start in [k*C, (k+1)*C) of the output; with units
     // of at most max_unit outputs and C >= max_unit every chunk is non-empty
     // and holds fewer than C + max_unit <= cap outputs.
-    uint64_t cap = max_chunk_nnz;
-    if (cap == 0) cap = std::min<uint64_t>(A.available() / 3 / 12, 1ull << 31);
+    // a chunk's output buffers (two when chunks overlap delivery) must fit
+    // the memory left; the caller's max_chunk_nnz can only lower that
+    uint64_t cap = std::min<uint64_t>(A.available() / 3 / 12, 1ull << 31);
+    if (max_chunk_nnz) cap = std::min(cap, max_chunk_nnz);
     cap = std::max<uint64_t>(cap, 1);
     struct Chunk {
         uint64_t lu0, lu1;  // light units [lu0, lu1)
@@ -1081,6 +1087,11 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
             gsparc_job &J = *G[j]->job;
             const uint64_t a0 = std::max(c0, job_first[j]), a1 = std::min(c1, job_first[j + 1]);
             if (a1 <= a0 || J.status != GSPARC_OK) continue;
+            if (G[j]->wide) {
+                // relabeled output keys back to x_f << Y_nfbits | y_f
+                wide_remap_keys(*G[j]->wide, out_k[bi].get() + (a0 - c0), a1 - a0, s2);
+                GS_CUDA(cudaStreamSynchronize(s2));
+            }
             deliver_slice(J.sink, out_k[bi].get() + (a0 - c0), out_v[bi].get() + (a0 - c0), a1 - a0,
                           a0 - job_first[j], job_nnz[j], s2, J.stats, bst.bytes_d2h);
         }
@@ -1166,6 +1177,8 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
             GS_REQUIRE(k.kind != GSPARC_SINK_DEVICE || k.on_chunk, GSPARC_EINVAL, "device sink needs on_chunk");
             Job q;
             q.job = &J;
+            q.tx = J.x;
+            q.ty = J.y;
             q.LX = make_layout(J.x->order, J.x->dims, J.ncmodes, J.cx);
             q.LY = make_layout(J.y->order, J.y->dims, J.ncmodes, J.cy);
             GS_REQUIRE(J.x->order > J.ncmodes && J.y->order > J.ncmodes, GSPARC_EUNSUPPORTED,
@@ -1173,20 +1186,28 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
             for (int m = 0; m < J.ncmodes; ++m)
                 GS_REQUIRE(q.LX.bits[J.cx[m]] == q.LY.bits[J.cy[m]], GSPARC_EINVAL,
                            "contract modes of X and Y have different bit widths (mode sizes differ)");
-            GS_REQUIRE(q.LX.nbits() <= 64 && q.LY.nbits() <= 64, GSPARC_EUNSUPPORTED, "operand keys wider than 64 bits");
             GS_REQUIRE(q.LX.nfbits + q.LY.nfbits <= 64, GSPARC_EUNSUPPORTED,
                        "output key wider than 64 bits (X free bits + Y free bits > 64)");
             GS_REQUIRE(J.x->nnz < kMaxGroupNnz && J.y->nnz < kMaxGroupNnz, GSPARC_EUNSUPPORTED,
                        "operand with more than 2^31 nonzeros");
+            const Layout LX0 = q.LX, LY0 = q.LY;
+            if (q.LX.nbits() > 64 || q.LY.nbits() > 64) {
+                // the reference's 128-bit key path: relabel onto 64-bit keys
+                q.wide = make_wide(ctx->arena, J.x, q.LX, J.y, q.LY, s);
+                q.tx = &q.wide->x2;
+                q.ty = &q.wide->y2;
+                q.LX = make_layout(2, q.tx->dims, 1, q.wide->cx2);
+                q.LY = make_layout(2, q.ty->dims, 1, q.wide->cy2);
+            }
             q.light_max = J.accum == GSPARC_ACCUM_DENSE ? 0 : kLightRowMax;
             q.width = std::max(q.LX.nbits(), q.LY.nbits());
             J.stats.nnz_x = J.x->nnz;
             J.stats.nnz_y = J.y->nnz;
-            J.stats.nbits_x = q.LX.nbits();
-            J.stats.nbits_y = q.LY.nbits();
-            J.stats.ncbits = q.LX.ncbits;
-            J.stats.nfbits_x = q.LX.nfbits;
-            J.stats.nfbits_y = q.LY.nfbits;
+            J.stats.nbits_x = LX0.nbits();
+            J.stats.nbits_y = LY0.nbits();
+            J.stats.ncbits = LX0.ncbits;
+            J.stats.nfbits_x = LX0.nfbits;
+            J.stats.nfbits_y = LY0.nfbits;
             J.stats.accumulator = J.accum;
             bst.nnz_x += J.x->nnz;
             bst.nnz_y += J.y->nnz;

@@ -18,6 +18,10 @@
  *   index match         include/gsparc/indexMatch.cuh:20-44,67-118,231-287
  *   ESC expand          include/gsparc/contraction.cuh:100-141 (key x_f<<Y_nfbits | y_f)
  *   sort + reduce       include/gsparc/contraction.cuh:506-537 (ascending keys, Sum)
+ *   keys over 64 bits   include/gsparc/tensor_manager.tpp:301-406 (ConvertTensor_extra:
+ *                       the same layouts in a 128-bit key), include/gsparc/indexMatch.cuh:
+ *                       120-229 (match on the full 128-bit contract key); output keys
+ *                       stay 64-bit (include/gsparc/contraction_extra.cuh)
  *
  * nnz follows the ESC semantics: every distinct output key that received at
  * least one product counts, including sums that cancel to exactly zero.
@@ -117,6 +121,67 @@ int oracle_linearize(int order, const uint64_t *dims, int nc, const int *cpos,
         keys[k] = role == 0 ? ((ncb >= 64 ? 0 : (f << ncb)) | c)
                             : ((nfb >= 64 ? 0 : (c << nfb)) | f);
     }
+    return OR_OK;
+}
+
+/*
+ * 128-bit keys (tensor_manager.tpp:301-406): the layouts above, in a key of
+ * up to 128 bits.  Used by oracle_sptc for every operand; keys of at most 64
+ * bits come out identical to oracle_linearize's.
+ */
+typedef unsigned __int128 u128;
+
+static void linearize128(int order, const int *shift, const int *isc, int ncb, int nfb,
+                         int role, uint64_t nnz, const uint64_t *idx, u128 *keys)
+{
+    for (uint64_t k = 0; k < nnz; ++k) {
+        u128 f = 0, c = 0;
+        for (int m = 0; m < order; ++m) {
+            u128 v = idx[(uint64_t)m * nnz + k];
+            if (isc[m])
+                c |= v << shift[m];
+            else
+                f |= v << shift[m];
+        }
+        keys[k] = role == 0 ? ((ncb >= 128 ? 0 : (f << ncb)) | c)
+                            : ((nfb >= 128 ? 0 : (c << nfb)) | f);
+    }
+}
+
+/* Stable LSD radix sort (16-bit digits) of 128-bit keys over their low nbits
+ * bits; perm receives the sorted order. */
+static int stable_sort_perm128(uint64_t n, const u128 *keys, int nbits, uint64_t *perm)
+{
+    uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * (n ? n : 1));
+    uint64_t *cnt = (uint64_t *)malloc(sizeof(uint64_t) * 65536);
+    if (!tmp || !cnt) {
+        free(tmp);
+        free(cnt);
+        return OR_ENOMEM;
+    }
+    for (uint64_t i = 0; i < n; ++i)
+        perm[i] = i;
+    uint64_t *a = perm, *b = tmp;
+    for (int sh = 0; sh < nbits; sh += 16) {
+        memset(cnt, 0, sizeof(uint64_t) * 65536);
+        for (uint64_t i = 0; i < n; ++i)
+            cnt[(uint64_t)(keys[a[i]] >> sh) & 0xFFFF]++;
+        uint64_t run = 0;
+        for (int d = 0; d < 65536; ++d) {
+            uint64_t c = cnt[d];
+            cnt[d] = run;
+            run += c;
+        }
+        for (uint64_t i = 0; i < n; ++i)
+            b[cnt[(uint64_t)(keys[a[i]] >> sh) & 0xFFFF]++] = a[i];
+        uint64_t *t = a;
+        a = b;
+        b = t;
+    }
+    if (a != perm)
+        memcpy(perm, a, sizeof(uint64_t) * n);
+    free(tmp);
+    free(cnt);
     return OR_OK;
 }
 
@@ -269,18 +334,22 @@ int oracle_sptc(int ox, const uint64_t *dx, uint64_t nx, const uint64_t *ix, con
     for (int i = 0; i < nc; ++i)
         if (oracle_mode_bits(dx[cx[i]]) != oracle_mode_bits(dy[cy[i]]))
             return OR_EINVAL;
-    if (ncx + nfx > 64 || ncy + nfy > 64 || nfx + nfy > 64)
+    /* operand keys of up to 128 bits (ConvertTensor_extra); output keys of 64 */
+    if (ncx + nfx > 128 || ncy + nfy > 128 || nfx + nfy > 64)
         return OR_EINVAL;
 
     oracle_result *r = (oracle_result *)calloc(1, sizeof(oracle_result));
-    uint64_t *kx = (uint64_t *)malloc(8 * (nx ? nx : 1));
-    uint64_t *ky = (uint64_t *)malloc(8 * (ny ? ny : 1));
+    u128 *kx = (u128 *)malloc(16 * (nx ? nx : 1));
+    u128 *ky = (u128 *)malloc(16 * (ny ? ny : 1));
+    u128 *kt = (u128 *)malloc(16 * ((nx > ny ? nx : ny) ? (nx > ny ? nx : ny) : 1));
     float *sx = (float *)malloc(4 * (nx ? nx : 1));
     float *sy = (float *)malloc(4 * (ny ? ny : 1));
+    float *st_ = (float *)malloc(4 * ((nx > ny ? nx : ny) ? (nx > ny ? nx : ny) : 1));
+    uint64_t *operm = (uint64_t *)malloc(8 * ((nx > ny ? nx : ny) ? (nx > ny ? nx : ny) : 1));
     uint64_t *pos = (uint64_t *)malloc(8 * (nx ? nx : 1));
     uint64_t *cnt = (uint64_t *)malloc(8 * (nx ? nx : 1));
     uint64_t *pre = (uint64_t *)malloc(8 * (nx + 1));
-    if (!r || !kx || !ky || !sx || !sy || !pos || !cnt || !pre) {
+    if (!r || !kx || !ky || !kt || !sx || !sy || !st_ || !operm || !pos || !cnt || !pre) {
         st = OR_ENOMEM;
         goto fail;
     }
@@ -288,15 +357,48 @@ int oracle_sptc(int ox, const uint64_t *dx, uint64_t nx, const uint64_t *ix, con
     r->y_nfbits = nfy;
     r->ncbits_x = ncx;
     r->ncbits_y = ncy;
-    oracle_linearize(ox, dx, nc, cx, 0, nx, ix, kx);
-    oracle_linearize(oy, dy, nc, cy, 1, ny, iy, ky);
-    memcpy(sx, vx, 4 * nx);
-    memcpy(sy, vy, 4 * ny);
-    if ((st = oracle_sort_pairs(nx, kx, sx, ncx + nfx)))
+    linearize128(ox, shx, iscx, ncx, nfx, 0, nx, ix, kx);
+    linearize128(oy, shy, iscy, ncy, nfy, 1, ny, iy, ky);
+    /* stable sort of each operand by its full key (sort.cuh:90-108) */
+    if ((st = stable_sort_perm128(nx, kx, ncx + nfx, operm)))
         goto fail;
-    if ((st = oracle_sort_pairs(ny, ky, sy, ncy + nfy)))
+    for (uint64_t i = 0; i < nx; ++i) {
+        kt[i] = kx[operm[i]];
+        st_[i] = vx[operm[i]];
+    }
+    memcpy(kx, kt, 16 * nx);
+    memcpy(sx, st_, 4 * nx);
+    if ((st = stable_sort_perm128(ny, ky, ncy + nfy, operm)))
         goto fail;
-    oracle_index_match(nx, kx, ncx, ny, ky, nfy, pos, cnt, pre);
+    for (uint64_t i = 0; i < ny; ++i) {
+        kt[i] = ky[operm[i]];
+        st_[i] = vy[operm[i]];
+    }
+    memcpy(ky, kt, 16 * ny);
+    memcpy(sy, st_, 4 * ny);
+    /* index match on the whole contract key (indexMatch.cuh:20-44,67-118,120-229) */
+    {
+        const u128 cmask = ncx >= 128 ? ~(u128)0 : (((u128)1 << ncx) - 1);
+        pre[0] = 0;
+        for (uint64_t i = 0; i < nx; ++i) {
+            const u128 c = kx[i] & cmask;
+            uint64_t lo = 0, hi = ny;
+            while (lo < hi) {
+                const uint64_t mid = lo + (hi - lo) / 2;
+                const u128 yc = nfy >= 128 ? 0 : (ky[mid] >> nfy);
+                if (yc < c)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            uint64_t n = 0;
+            while (lo + n < ny && (nfy >= 128 ? 0 : (ky[lo + n] >> nfy)) == c)
+                ++n;
+            pos[i] = n ? lo : 0;
+            cnt[i] = n;
+            pre[i + 1] = pre[i] + n;
+        }
+    }
     uint64_t ir = pre[nx];
     r->ir_nnz = ir;
     if (ir > max_products) {
@@ -317,9 +419,9 @@ int oracle_sptc(int ox, const uint64_t *dx, uint64_t nx, const uint64_t *ix, con
         uint64_t fmask = nfy >= 64 ? ~0ull : ((1ull << nfy) - 1);
         uint64_t p = 0;
         for (uint64_t i = 0; i < nx; ++i) {
-            uint64_t xf = ncx >= 64 ? 0 : (kx[i] >> ncx);
+            uint64_t xf = (uint64_t)(kx[i] >> ncx);  /* nfx <= 64 bits */
             for (uint64_t j = 0; j < cnt[i]; ++j) {
-                uint64_t yk = ky[pos[i] + j];
+                uint64_t yk = (uint64_t)ky[pos[i] + j];
                 pk[p] = (nfy >= 64 ? 0 : (xf << nfy)) | (yk & fmask);
                 pv[p] = (double)sx[i] * (double)sy[pos[i] + j];
                 ++p;
@@ -369,8 +471,11 @@ int oracle_sptc(int ox, const uint64_t *dx, uint64_t nx, const uint64_t *ix, con
     }
     free(kx);
     free(ky);
+    free(kt);
     free(sx);
     free(sy);
+    free(st_);
+    free(operm);
     free(pos);
     free(cnt);
     free(pre);
@@ -379,8 +484,11 @@ int oracle_sptc(int ox, const uint64_t *dx, uint64_t nx, const uint64_t *ix, con
 fail:
     free(kx);
     free(ky);
+    free(kt);
     free(sx);
     free(sy);
+    free(st_);
+    free(operm);
     free(pos);
     free(cnt);
     free(pre);

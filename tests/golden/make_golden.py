@@ -65,12 +65,24 @@ def dense_like():
     return X, Y, [1, 2], [0, 1]
 
 
+def wide_keys():
+    # X keys of 65 bits (free modes 2^17 x 2^17, contract modes 2^16 x 2^15):
+    # the reference's 128-bit key path (ConvertTensor_extra); output keys of
+    # 34 + 13 = 47 bits.  The contract space stays below 2^32 because the
+    # baseline built here packs contract coordinates into 32-bit indices.
+    X = synth.make_tensor([1 << 17, 1 << 17, 1 << 16, 1 << 15], 2000,
+                          ["uniform", "uniform", ("zipf", 1.3), ("zipf", 1.3)], "u11", 41)
+    Y = synth.make_tensor([1 << 16, 1 << 15, 5000], 2000, [("zipf", 1.3), ("zipf", 1.3), "uniform"], "u11", 42)
+    return X, Y, [2, 3], [0, 1]
+
+
 CASES = {
     "plain_small_s002": lambda: synth.plain_small(scale=0.02, seed=0),
     "esc_large_s0005": lambda: synth.esc_large(scale=0.0005, seed=1),
     "dense_like": dense_like,
     "mixed_orders": mixed_orders,
     "reordered_cmodes": reordered_cmodes,
+    "wide_keys": wide_keys,
 }
 
 

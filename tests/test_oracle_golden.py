@@ -46,3 +46,27 @@ def test_oracle_layout_follows_reference_mask_order():
 def test_oracle_size_one_mode_takes_zero_bits():
     assert ob.mode_bits(1) == 0 and ob.mode_bits(2) == 1 and ob.mode_bits(1024) == 10
     assert ob.mode_bits(1025) == 11 and ob.mode_bits(2**64 - 1) == 64
+
+
+def test_oracle_wide_contract_keys_match_coordinate_sums():
+    """Contract keys of 66 bits (the reference's 128-bit path): the oracle's
+    128-bit keys against a plain dictionary contraction over coordinates."""
+    from collections import defaultdict
+    from gsparc_b200 import synth
+    d = 1 << 22
+    X = synth.make_tensor([300, d, d, d], 600, ["uniform"] + [("zipf", 1.6)] * 3, "u11", 3)
+    Y = synth.make_tensor([d, d, d, 200], 600, [("zipf", 1.6)] * 3 + ["uniform"], "u11", 4)
+    ymap = defaultdict(list)
+    for k in range(Y.nnz):
+        ymap[tuple(int(Y.idx[m][k]) for m in (0, 1, 2))].append((int(Y.idx[3][k]), float(Y.val[k])))
+    ref = defaultdict(float)
+    for k in range(X.nnz):
+        for yf, yv in ymap.get(tuple(int(X.idx[m][k]) for m in (1, 2, 3)), []):
+            ref[(int(X.idx[0][k]), yf)] += float(X.val[k]) * yv
+    z = ob.sptc(X, Y, [1, 2, 3], [0, 1, 2])
+    coords = ob.decode_keys(z.keys, X, Y, [1, 2, 3], [0, 1, 2])
+    got = {(int(a), int(b)): v for a, b, v in zip(coords[0], coords[1], z.vals)}
+    assert z.nnz == len(ref) > 0
+    assert sorted(got) == sorted(ref)
+    for k, v in ref.items():
+        assert abs(got[k] - v) <= 1e-9 * max(1.0, abs(v))
