@@ -86,7 +86,8 @@ EXPORTS = [
     "gsparc_sort_pairs", "gsparc_index_match", "gsparc_digest_chunk", "gsparc_sptc_batch",
     "gsparc_serve_create", "gsparc_serve_destroy", "gsparc_serve_upload", "gsparc_serve_release",
     "gsparc_serve_submit", "gsparc_serve_poll", "gsparc_serve_wait", "gsparc_serve_stats",
-    "gsparc_serve_reset_stats",
+    "gsparc_serve_reset_stats", "gsparc_sptc_resident", "gsparc_tensor_download",
+    "gsparc_read_quantum",
 ]
 
 
@@ -142,10 +143,12 @@ def lib():
     L.gsparc_tensor_upload.argtypes = [P, ctypes.POINTER(_Coo), P, ctypes.POINTER(P)]
     L.gsparc_tensor_free.argtypes = [P, P]
     L.gsparc_tensor_info.argtypes = [P, P, P, P]
+    L.gsparc_tensor_download.argtypes = [P, P, P, P]
     L.gsparc_sptc.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(_Sink), ctypes.POINTER(Stats), P]
     L.gsparc_sptc_shard.argtypes = [P, P, P, I, P, P, I, I, I, ctypes.POINTER(_Sink),
                                     ctypes.POINTER(Stats), P]
     L.gsparc_read_tns.argtypes = [ctypes.c_char_p, I, P, P, P, ctypes.POINTER(P), ctypes.POINTER(P)]
+    L.gsparc_read_quantum.argtypes = [ctypes.c_char_p, I, P, P, P, ctypes.POINTER(P), ctypes.POINTER(P)]
     L.gsparc_write_tns.argtypes = [ctypes.c_char_p, I, U64, P, P]
     L.gsparc_free_host.argtypes = [P]
     L.gsparc_layout.argtypes = [I, P, I, P, P, P, P, P, P]
@@ -155,6 +158,7 @@ def lib():
     L.gsparc_index_match.argtypes = [P, U64, P, I, U64, P, I, P, P, P, P, P]
     L.gsparc_digest_chunk.argtypes = [P, P, U64, ctypes.POINTER(Digest), P]
     L.gsparc_sptc_batch.argtypes = [P, P, I, U64, ctypes.POINTER(Stats), P]
+    L.gsparc_sptc_resident.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(P), ctypes.POINTER(Stats), P]
     L.gsparc_serve_create.argtypes = [I, ctypes.POINTER(_ServerOpts), ctypes.POINTER(P)]
     L.gsparc_serve_destroy.argtypes = [P]
     L.gsparc_serve_upload.argtypes = [P, ctypes.POINTER(_Coo), ctypes.POINTER(P)]
@@ -203,12 +207,22 @@ def layout(dims: Sequence[int], cmodes: Sequence[int]):
 
 
 def read_tns(path: str, nthreads: int = 0) -> CooTensor:
+    return _read(lib().gsparc_read_tns, path, nthreads)
+
+
+def read_quantum(path: str, nthreads: int = 0) -> CooTensor:
+    """Quantum-chemistry directory (indices.txt + values.txt), the reference's -q
+    (IOManager::_ReadQuantumData, include/gsparc/io_manager.tpp:310-484)."""
+    return _read(lib().gsparc_read_quantum, path, nthreads)
+
+
+def _read(fn, path: str, nthreads: int) -> CooTensor:
     order = np.zeros(1, np.int32)
     dims = np.zeros(32, np.uint64)
     nnz = np.zeros(1, np.uint64)
     pidx, pval = ctypes.c_void_p(), ctypes.c_void_p()
-    _check(lib().gsparc_read_tns(path.encode(), nthreads, _p(order), _p(dims), _p(nnz),
-                                 ctypes.byref(pidx), ctypes.byref(pval)), f"read_tns({path})")
+    _check(fn(path.encode(), nthreads, _p(order), _p(dims), _p(nnz), ctypes.byref(pidx), ctypes.byref(pval)),
+           f"read({path})")
     o, n = int(order[0]), int(nnz[0])
     try:
         idx = np.ctypeslib.as_array(ctypes.cast(pidx, ctypes.POINTER(ctypes.c_uint64)),
@@ -310,6 +324,13 @@ class DeviceTensor:
     def handle(self):
         return self._h
 
+    def download(self) -> CooTensor:
+        """Copy the tensor back to host memory."""
+        idx = np.zeros((self.order, self.nnz), np.uint64)
+        val = np.zeros(self.nnz, np.float32)
+        _check(lib().gsparc_tensor_download(self._h, _p(idx), _p(val), None), "tensor_download")
+        return CooTensor(list(self.dims), idx, val)
+
     def free(self):
         if self._h:
             _check(lib().gsparc_tensor_free(self.ctx.handle, self._h), "tensor_free")
@@ -410,6 +431,39 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
             keys = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0, np.uint64)
             vals = np.concatenate([p[2] for p in parts]) if parts else np.zeros(0, np.float32)
     return SpTCResult(int(st.nnz), int(st.ir_nnz), keys, vals, st.as_dict())
+
+
+class ResidentResult(DeviceTensor):
+    """A contraction result kept on the device (gsparc_sptc_resident): a
+    COO operand whose modes are X's free modes then Y's free modes."""
+
+    def __init__(self, ctx: Context, handle, stats: dict):
+        self.ctx = ctx
+        self._h = handle
+        self.stats = stats
+        order = ctypes.c_int()
+        dims = np.zeros(32, np.uint64)
+        nnz = ctypes.c_uint64()
+        _check(lib().gsparc_tensor_info(handle, ctypes.byref(order), _p(dims), ctypes.byref(nnz)), "tensor_info")
+        self.order = order.value
+        self.dims = [int(d) for d in dims[: self.order]]
+        self.nnz = nnz.value
+
+
+def sptc_resident(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: Sequence[int],
+                  dense_accumulator: int = ACCUM_AUTO, stream: int = 0) -> ResidentResult:
+    """Z = X x_{cx,cy} Y kept resident, usable as an operand of further
+    contractions (the reference's multi-SpTC chaining)."""
+    if len(cx) != len(cy):
+        raise ValueError("cx and cy must have the same length")
+    c1 = np.asarray(cx, np.int32)
+    c2 = np.asarray(cy, np.int32)
+    st = Stats()
+    h = ctypes.c_void_p()
+    _check(lib().gsparc_sptc_resident(ctx.handle, X.handle, Y.handle, len(c1), _p(c1), _p(c2),
+                                      int(dense_accumulator), ctypes.byref(h), ctypes.byref(st),
+                                      ctypes.c_void_p(stream)), "sptc_resident")
+    return ResidentResult(ctx, h, st.as_dict())
 
 
 def sptc_batch(ctx: Context, jobs, sink: str = "host", max_chunk_nnz: int = 0, stream: int = 0,

@@ -168,6 +168,19 @@ gsparc_status gsparc_tensor_free(gsparc_ctx *ctx, gsparc_tensor *t) {
     });
 }
 
+gsparc_status gsparc_tensor_download(const gsparc_tensor *t, uint64_t *idx, float *val, void *stream) {
+    return guard([&] {
+        GS_REQUIRE(t && (t->nnz == 0 || (idx && val)), GSPARC_EINVAL, "null argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        const uint64_t n = t->nnz;
+        if (n) {
+            GS_CUDA(cudaMemcpyAsync(idx, t->d_idx, 8 * (size_t)t->order * n, cudaMemcpyDeviceToHost, s));
+            GS_CUDA(cudaMemcpyAsync(val, t->d_val, 4 * n, cudaMemcpyDeviceToHost, s));
+        }
+        GS_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 gsparc_status gsparc_tensor_info(const gsparc_tensor *t, int *order, uint64_t *dims, uint64_t *nnz) {
     return guard([&] {
         GS_REQUIRE(t, GSPARC_EINVAL, "null tensor");
@@ -224,6 +237,16 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
     });
 }
 
+gsparc_status gsparc_sptc_resident(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int ncmodes,
+                                   const int *cx, const int *cy, int accum, gsparc_tensor **Z,
+                                   gsparc_stats *stats, void *stream) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        DeviceScope ds(ctx->device);
+        gs::sptc_resident(ctx, X, Y, ncmodes, cx, cy, accum, Z, stats, (cudaStream_t)stream);
+    });
+}
+
 gsparc_status gsparc_sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz,
                                 gsparc_stats *stats, void *stream) {
     return guard([&] {
@@ -238,6 +261,14 @@ gsparc_status gsparc_read_tns(const char *path, int nthreads, int *order, uint64
     return guard([&] {
         GS_REQUIRE(path && order && dims && nnz && idx && val, GSPARC_EINVAL, "null argument");
         gs::read_tns(path, nthreads, order, dims, nnz, idx, val);
+    });
+}
+
+gsparc_status gsparc_read_quantum(const char *dir, int nthreads, int *order, uint64_t *dims, uint64_t *nnz,
+                                  uint64_t **idx, float **val) {
+    return guard([&] {
+        GS_REQUIRE(dir && order && dims && nnz && idx && val, GSPARC_EINVAL, "null argument");
+        gs::read_quantum(dir, nthreads, order, dims, nnz, idx, val);
     });
 }
 

@@ -4,8 +4,13 @@
 // (reference: src/gsparc/cmdline_opts.cpp:9-193, main.cu:22-437):
 //   gsparc -X x.tns -Y y.tns -c N -x m1 .. mN -y m1 .. mN [-g G] [-n iters] [-d 1|0|-1]
 // Extension: -o z.tns writes the output tensor (1-based, %.9g values).
-// Not supported here (they are separate features of the reference): -q
-// (quantum directory input) and -m/-a/-z (chained multi-SpTC).
+// Chained multi-SpTC (-m 1 -a N -z m1 .. mN, main.cu:323-371): Z1 = X x Y stays
+// on the device, then Z = Z1 x T with T the tensor of the -Y file (the
+// reference parses it a second time for this, main.cu:42-48), contracting
+// Z1's last N modes (Y's free modes, the low bits of the reference's Z1 keys
+// that its second contraction matches on) with modes m1..mN of T.
+// -q reads both operands from the quantum directory format (indices.txt +
+// values.txt, io_manager.tpp:310-484).
 #include <getopt.h>
 
 #include <chrono>
@@ -28,6 +33,8 @@ struct Opts {
     int gpus = 1, iters = 1, dense = 0;
     bool quantum = false;
     int multi = 0;
+    int na = 0;
+    std::vector<int> cz;
 };
 
 [[noreturn]] void die(const char *what, gsparc_status st) {
@@ -37,7 +44,8 @@ struct Opts {
 
 void usage(const char *argv0) {
     std::fprintf(stderr,
-                 "Usage: %s -X x.tns -Y y.tns -c N -x m1..mN -y m1..mN [-g G] [-n iters] [-d 1|0|-1] [-o z.tns]\n",
+                 "Usage: %s -X x.tns -Y y.tns -c N -x m1..mN -y m1..mN [-g G] [-n iters] [-d 1|0|-1] [-q]\n"
+                 "          [-m 1 -a K -z t1..tK] [-o z.tns]\n",
                  argv0);
 }
 
@@ -66,6 +74,122 @@ int collect_chunk(void *user, const uint64_t *k, const float *v, uint64_t n, uin
     return 0;
 }
 
+// The reference's stderr report (main.cu:415-432); times in seconds.
+void print_report(double slitom, double idxmatch, double contraction, double dprtn, uint64_t result_nnz,
+                  int iters) {
+    const double partition = 0.0;
+    const double n = iters;
+    const double total = slitom + partition + idxmatch + contraction + dprtn;
+    std::fprintf(stderr, "--------Break Down--------\n");
+    std::fprintf(stderr, "SLITOM time: %f\n", slitom / n);
+    std::fprintf(stderr, "Partition time: %f\n", partition / n);
+    std::fprintf(stderr, "Idxmatch time: %f\n", idxmatch / n);
+    std::fprintf(stderr, "Contraction time: %f\n", contraction / n);
+    std::fprintf(stderr, "Dynamic Partition time: %f\n", dprtn / n);
+    std::fprintf(stderr, "--------Elapsed Time--------\n");
+    std::fprintf(stderr, "Result NNZ: %llu\n", (unsigned long long)(result_nnz / iters));
+    std::fprintf(stderr, "SLITOM time: %f\n", slitom / n);
+    std::fprintf(stderr, "Partition time: %f\n", partition / n);
+    std::fprintf(stderr, "SpTC(IdxMatch + Contraction + Data Copy) time: %f\n", (idxmatch + contraction + dprtn) / n);
+    std::fprintf(stderr, "Total time: %f\n", total / n);
+    std::fprintf(stderr, "\n\n");
+}
+
+// Output keys -> coordinates (X free modes ascending, then Y free modes), written as .tns.
+void write_output(const std::string &path, const OutCollect &out, int xo, const uint64_t *xd, const int *cx,
+                  int yo, const uint64_t *yd, const int *cy, int nc) {
+    int bx[32], shx[32], icx[32], ncx, nfx, by[32], shy[32], icy[32], ncy, nfy;
+    gsparc_layout(xo, xd, nc, cx, bx, shx, icx, &ncx, &nfx);
+    gsparc_layout(yo, yd, nc, cy, by, shy, icy, &ncy, &nfy);
+    std::vector<int> fmx, fmy;
+    for (int m = 0; m < xo; ++m) if (!icx[m]) fmx.push_back(m);
+    for (int m = 0; m < yo; ++m) if (!icy[m]) fmy.push_back(m);
+    const int zo = (int)(fmx.size() + fmy.size());
+    const uint64_t zn = out.keys.size();
+    std::vector<uint64_t> zi((size_t)zo * zn);
+    for (uint64_t k = 0; k < zn; ++k) {
+        uint64_t key = out.keys[k];
+        uint64_t xf = nfy >= 64 ? 0 : key >> nfy;
+        uint64_t yf = nfy >= 64 ? key : key & ((1ull << nfy) - 1);
+        int z = 0;
+        for (int m : fmx) zi[(size_t)(z++) * zn + k] = (xf >> shx[m]) & ((bx[m] >= 64) ? ~0ull : ((1ull << bx[m]) - 1));
+        for (int m : fmy) zi[(size_t)(z++) * zn + k] = (yf >> shy[m]) & ((by[m] >= 64) ? ~0ull : ((1ull << by[m]) - 1));
+    }
+    gsparc_status st = gsparc_write_tns(path.c_str(), zo, zn, zi.data(), out.vals.data());
+    if (st) die("writing Z", st);
+}
+
+// -m: Z1 = X x Y kept on the device, then Z = Z1 x T (T = the -Y tensor),
+// Z1's last N modes against T's modes -z m1..mN.  One GPU.
+int run_multi(const Opts &o, const Tensor &tx, const Tensor &ty) {
+    if (o.gpus != 1) {
+        std::fprintf(stderr, "gsparc: chained multi-SpTC (-m) runs on one GPU (-g 1)\n");
+        return 1;
+    }
+    const int yfree = ty.order - o.nc;
+    if (o.na < 1 || o.na > yfree || (int)o.cz.size() != o.na) {
+        std::fprintf(stderr, "gsparc: -m needs -a N (1..%d, Y's free modes) and -z with N modes of the -Y tensor\n",
+                     yfree);
+        return 1;
+    }
+    double slitom = 0, idxmatch = 0, contraction = 0, dprtn = 0, first = 0;
+    uint64_t result_nnz = 0;
+    OutCollect out;
+    int z1o = 0;
+    uint64_t z1d[32] = {};
+    std::vector<int> cz1(o.na);
+    for (int it = 0; it < o.iters; ++it) {
+        gsparc_ctx *ctx = nullptr;
+        gsparc_status s = gsparc_ctx_create(0, 0, &ctx);
+        if (s) die("context", s);
+        const uint64_t *ix[32], *iy[32];
+        for (int m = 0; m < tx.order; ++m) ix[m] = tx.idx + (size_t)m * tx.nnz;
+        for (int m = 0; m < ty.order; ++m) iy[m] = ty.idx + (size_t)m * ty.nnz;
+        gsparc_coo cx{tx.order, tx.dims, tx.nnz, ix, tx.val, 0};
+        gsparc_coo cy{ty.order, ty.dims, ty.nnz, iy, ty.val, 0};
+        gsparc_tensor *X = nullptr, *Y = nullptr, *Z1 = nullptr;
+        auto t0 = std::chrono::steady_clock::now();
+        if ((s = gsparc_tensor_upload(ctx, &cx, nullptr, &X)) || (s = gsparc_tensor_upload(ctx, &cy, nullptr, &Y)))
+            die("upload", s);
+        const double up = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        gsparc_stats s1{}, s2{};
+        s = gsparc_sptc_resident(ctx, X, Y, o.nc, o.cx.data(), o.cy.data(), o.dense, &Z1, &s1, nullptr);
+        if (s) die("first contraction", s);
+        first += (up + s1.t_linearize_ms + s1.t_sort_ms + s1.t_match_ms + s1.t_plan_ms + s1.t_contract_ms) / 1e3;
+        gsparc_tensor_info(Z1, &z1o, z1d, nullptr);
+        for (int i = 0; i < o.na; ++i) cz1[i] = z1o - o.na + i;
+        gsparc_sink sink{};
+        sink.kind = GSPARC_SINK_DISCARD;
+        std::vector<uint64_t> hk;
+        std::vector<float> hv;
+        if (!o.out.empty() && it == 0) {
+            sink.kind = GSPARC_SINK_HOST;
+            hk.resize(1 << 24);
+            hv.resize(1 << 24);
+            sink.host_keys = hk.data();
+            sink.host_vals = hv.data();
+            sink.host_capacity = hk.size();
+            sink.on_chunk = collect_chunk;
+            sink.user = &out;
+        }
+        s = gsparc_sptc(ctx, Z1, Y, o.na, cz1.data(), o.cz.data(), o.dense, &sink, &s2, nullptr);
+        if (s) die("second contraction", s);
+        result_nnz += s2.nnz;
+        slitom += (up + s1.t_linearize_ms + s1.t_sort_ms + s2.t_linearize_ms + s2.t_sort_ms) / 1e3;
+        idxmatch += (s1.t_match_ms + s2.t_match_ms) / 1e3;
+        dprtn += (s1.t_plan_ms + s2.t_plan_ms) / 1e3;
+        contraction += (s1.t_contract_ms + s2.t_contract_ms) / 1e3;
+        gsparc_tensor_free(ctx, Z1);
+        gsparc_tensor_free(ctx, X);
+        gsparc_tensor_free(ctx, Y);
+        gsparc_ctx_destroy(ctx);
+    }
+    std::fprintf(stderr, "First SpTC time: %f\n", first / o.iters);
+    print_report(slitom, idxmatch, contraction, dprtn, result_nnz, o.iters);
+    if (!o.out.empty()) write_output(o.out, out, z1o, z1d, cz1.data(), ty.order, ty.dims, o.cz.data(), o.na);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -84,22 +208,30 @@ int main(int argc, char **argv) {
         case 'c':
             o.nc = std::atoi(optarg);
             break;
+        case 'a':
+            o.na = std::atoi(optarg);
+            break;
         case 'x':
-        case 'y': {
-            // the modes follow the flag as separate arguments (cmdline_opts.cpp:112-139)
-            std::vector<int> &v = c == 'x' ? o.cx : o.cy;
-            std::fprintf(stderr, "# contract modes of %c: %d, contract modes: ", c == 'x' ? 'X' : 'Y', o.nc);
+        case 'y':
+        case 'z': {
+            // the modes follow the flag as separate arguments (cmdline_opts.cpp:112-139,140-155)
+            std::vector<int> &v = c == 'x' ? o.cx : (c == 'y' ? o.cy : o.cz);
+            const int k = c == 'z' ? o.na : o.nc;
+            if (c == 'z')
+                std::fprintf(stderr, "# contract modes of Z (second SpTC): %d, contract modes: ", k);
+            else
+                std::fprintf(stderr, "# contract modes of %c: %d, contract modes: ", c == 'x' ? 'X' : 'Y', k);
             v.clear();
-            for (int i = 0; i < o.nc; ++i) {
+            for (int i = 0; i < k; ++i) {
                 if (optind - 1 + i >= argc) {
-                    std::fprintf(stderr, "\ngsparc: -%c needs %d modes\n", c, o.nc);
+                    std::fprintf(stderr, "\ngsparc: -%c needs %d modes\n", c, k);
                     return 1;
                 }
                 v.push_back(std::atoi(argv[optind - 1 + i]));
                 std::fprintf(stderr, "%d ", v.back());
             }
             std::fprintf(stderr, "\n");
-            optind += o.nc - 1;
+            optind += k - 1;
             break;
         }
         case 'g':
@@ -121,9 +253,8 @@ int main(int argc, char **argv) {
             break;
         case 'm':
             o.multi = std::atoi(optarg);
+            std::fprintf(stderr, "multi_sptc: %d\n", o.multi);
             break;
-        case 'a':
-        case 'z':
         case 'b':
         case 'v':
             break;
@@ -135,14 +266,6 @@ int main(int argc, char **argv) {
             return 1;
         }
     }
-    if (o.quantum) {
-        std::fprintf(stderr, "gsparc: the quantum input format (-q) is not supported by this build\n");
-        return 1;
-    }
-    if (o.multi) {
-        std::fprintf(stderr, "gsparc: chained multi-SpTC (-m) is not supported by this build\n");
-        return 1;
-    }
     if (o.X.empty() || o.Y.empty() || o.nc < 1 || (int)o.cx.size() != o.nc || (int)o.cy.size() != o.nc ||
         o.gpus < 1 || o.iters < 1 || o.dense < -1 || o.dense > 1) {
         usage(argv[0]);
@@ -150,10 +273,20 @@ int main(int argc, char **argv) {
     }
 
     Tensor tx, ty;
-    gsparc_status st = gsparc_read_tns(o.X.c_str(), 0, &tx.order, tx.dims, &tx.nnz, &tx.idx, &tx.val);
+    // -q: both operands in the quantum directory format (main.cu:44-48)
+    auto rd = o.quantum ? gsparc_read_quantum : gsparc_read_tns;
+    gsparc_status st = rd(o.X.c_str(), 0, &tx.order, tx.dims, &tx.nnz, &tx.idx, &tx.val);
     if (st) die("reading X", st);
-    st = gsparc_read_tns(o.Y.c_str(), 0, &ty.order, ty.dims, &ty.nnz, &ty.idx, &ty.val);
+    st = rd(o.Y.c_str(), 0, &ty.order, ty.dims, &ty.nnz, &ty.idx, &ty.val);
     if (st) die("reading Y", st);
+    if (o.multi) {
+        const int rc = run_multi(o, tx, ty);
+        gsparc_free_host(tx.idx);
+        gsparc_free_host(tx.val);
+        gsparc_free_host(ty.idx);
+        gsparc_free_host(ty.val);
+        return rc;
+    }
 
     double slitom = 0, idxmatch = 0, contraction = 0, dprtn = 0;
     uint64_t result_nnz = 0;
@@ -224,45 +357,8 @@ int main(int argc, char **argv) {
         }
     }
 
-    const double partition = 0.0;
-    const double n = o.iters;
-    const double total = slitom + partition + idxmatch + contraction + dprtn;
-    std::fprintf(stderr, "--------Break Down--------\n");
-    std::fprintf(stderr, "SLITOM time: %f\n", slitom / n);
-    std::fprintf(stderr, "Partition time: %f\n", partition / n);
-    std::fprintf(stderr, "Idxmatch time: %f\n", idxmatch / n);
-    std::fprintf(stderr, "Contraction time: %f\n", contraction / n);
-    std::fprintf(stderr, "Dynamic Partition time: %f\n", dprtn / n);
-    std::fprintf(stderr, "--------Elapsed Time--------\n");
-    std::fprintf(stderr, "Result NNZ: %llu\n", (unsigned long long)(result_nnz / o.iters));
-    std::fprintf(stderr, "SLITOM time: %f\n", slitom / n);
-    std::fprintf(stderr, "Partition time: %f\n", partition / n);
-    std::fprintf(stderr, "SpTC(IdxMatch + Contraction + Data Copy) time: %f\n", (idxmatch + contraction + dprtn) / n);
-    std::fprintf(stderr, "Total time: %f\n", total / n);
-    std::fprintf(stderr, "\n\n");
-
-    if (!o.out.empty()) {
-        // decode keys into coordinates: X free modes ascending, then Y free modes
-        int bx[32], shx[32], icx[32], ncx, nfx, by[32], shy[32], icy[32], ncy, nfy;
-        gsparc_layout(tx.order, tx.dims, o.nc, o.cx.data(), bx, shx, icx, &ncx, &nfx);
-        gsparc_layout(ty.order, ty.dims, o.nc, o.cy.data(), by, shy, icy, &ncy, &nfy);
-        std::vector<int> fmx, fmy;
-        for (int m = 0; m < tx.order; ++m) if (!icx[m]) fmx.push_back(m);
-        for (int m = 0; m < ty.order; ++m) if (!icy[m]) fmy.push_back(m);
-        const int zo = (int)(fmx.size() + fmy.size());
-        const uint64_t zn = out.keys.size();
-        std::vector<uint64_t> zi((size_t)zo * zn);
-        for (uint64_t k = 0; k < zn; ++k) {
-            uint64_t key = out.keys[k];
-            uint64_t xf = nfy >= 64 ? 0 : key >> nfy;
-            uint64_t yf = nfy >= 64 ? key : key & ((1ull << nfy) - 1);
-            int z = 0;
-            for (int m : fmx) zi[(size_t)(z++) * zn + k] = (xf >> shx[m]) & ((bx[m] >= 64) ? ~0ull : ((1ull << bx[m]) - 1));
-            for (int m : fmy) zi[(size_t)(z++) * zn + k] = (yf >> shy[m]) & ((by[m] >= 64) ? ~0ull : ((1ull << by[m]) - 1));
-        }
-        st = gsparc_write_tns(o.out.c_str(), zo, zn, zi.data(), out.vals.data());
-        if (st) die("writing Z", st);
-    }
+    print_report(slitom, idxmatch, contraction, dprtn, result_nnz, o.iters);
+    if (!o.out.empty()) write_output(o.out, out, tx.order, tx.dims, o.cx.data(), ty.order, ty.dims, o.cy.data(), o.nc);
     gsparc_free_host(tx.idx);
     gsparc_free_host(tx.val);
     gsparc_free_host(ty.idx);

@@ -21,11 +21,17 @@ using JobDoneFn = std::function<void(gsparc_job *)>;
 void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st,
                 cudaStream_t s, int shard = 0, int nshards = 1, const JobDoneFn *done_fn = nullptr);
 
+// Z = X x Y decoded into a resident COO tensor (chain.cu).
+void sptc_resident(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int nc, const int *cx,
+                   const int *cy, int accum, gsparc_tensor **out, gsparc_stats *stats, cudaStream_t s);
+
 void plan_shards(const uint64_t *row_prod, uint64_t nrows, int nshards, uint64_t *bounds);
 
 // .tns text I/O (tns_io.cpp)
 void read_tns(const char *path, int nthreads, int *order, uint64_t *dims, uint64_t *nnz,
               uint64_t **idx, float **val);
 void write_tns(const char *path, int order, uint64_t nnz, const uint64_t *idx, const float *val);
+void read_quantum(const char *dir, int nthreads, int *order, uint64_t *dims, uint64_t *nnz, uint64_t **idx,
+                  float **val);
 
 }  // namespace gs

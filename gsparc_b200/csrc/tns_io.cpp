@@ -185,6 +185,125 @@ void read_tns(const char *path, int nthreads, int *order_out, uint64_t *dims_out
     *val_out = val;
 }
 
+// Quantum-chemistry directory format (reference: include/gsparc/io_manager.tpp:
+// 310-484, the -q flag): <dir>/indices.txt holds one line per mode with the
+// 1-based indices of all nonzeros of that mode, <dir>/values.txt the nnz
+// values.  The order is the number of index lines, nnz the number of tokens
+// of a line, dims[m] the largest index of mode m.  Indices are parsed as
+// numbers (the reference uses strtod, so "3.0" is index 3).  Unlike the
+// reference, values are parsed as double and narrowed to float (it scans
+// "%le" into a float slot), blank lines are skipped, and lines of different
+// lengths, non-integral or non-positive indices and missing values are
+// reported instead of being read past.
+void read_quantum(const char *dir, int nthreads, int *order_out, uint64_t *dims_out, uint64_t *nnz_out,
+                  uint64_t **idx_out, float **val_out) {
+    auto slurp = [](const std::string &p) {
+        FILE *f = std::fopen(p.c_str(), "rb");
+        if (!f) fail(GSPARC_EIO, "cannot open " + p);
+        std::fseek(f, 0, SEEK_END);
+        long sz = std::ftell(f);
+        std::rewind(f);
+        std::vector<char> d((size_t)std::max<long>(sz, 0) + 1, '\0');
+        if (sz > 0 && std::fread(d.data(), 1, (size_t)sz, f) != (size_t)sz) {
+            std::fclose(f);
+            fail(GSPARC_EIO, "short read of " + p);
+        }
+        std::fclose(f);
+        d[(size_t)std::max<long>(sz, 0)] = '\0';
+        return d;
+    };
+    const std::string base(dir);
+    std::vector<char> ib = slurp(base + "/indices.txt");
+    std::vector<char> vb = slurp(base + "/values.txt");
+    // index lines holding a token
+    std::vector<Span> lines;
+    {
+        const size_t n = ib.size() - 1;
+        size_t i = 0;
+        while (i < n) {
+            size_t j = i;
+            bool tok = false;
+            while (j < n && ib[j] != '\n') {
+                if (!is_sep(ib[j])) tok = true;
+                ++j;
+            }
+            if (tok) lines.push_back({i, j});
+            i = j + 1;
+        }
+    }
+    const int order = (int)lines.size();
+    GS_REQUIRE(order >= 1 && order <= kMaxOrder, GSPARC_EIO, "indices.txt must hold 1..32 non-empty lines");
+    for (auto &l : lines) ib[l.e] = '\0';  // each line ends its own string
+    std::vector<std::vector<uint64_t>> rows(order);
+    std::vector<std::string> errs(order);
+    auto parse_row = [&](int m) {
+        const char *p = ib.data() + lines[m].b;
+        std::vector<uint64_t> &r = rows[m];
+        for (;;) {
+            while (*p && is_sep(*p)) ++p;
+            if (!*p) break;
+            char *end = nullptr;
+            errno = 0;
+            const double v = std::strtod(p, &end);
+            if (end == p || errno || !(v >= 1.0) || v != (double)(uint64_t)v || v > 9.007199254740992e15) {
+                errs[m] = "bad index on line " + std::to_string(m + 1) + " of indices.txt";
+                return;
+            }
+            r.push_back((uint64_t)v - 1);
+            p = end;
+        }
+    };
+    if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+    {
+        std::vector<std::thread> th;
+        const int nt = std::min(nthreads, order);
+        for (int t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                for (int m = t; m < order; m += nt) parse_row(m);
+            });
+        for (auto &x : th) x.join();
+    }
+    for (int m = 0; m < order; ++m) GS_REQUIRE(errs[m].empty(), GSPARC_EIO, errs[m]);
+    const uint64_t nnz = rows[0].size();
+    for (int m = 1; m < order; ++m)
+        GS_REQUIRE(rows[m].size() == nnz, GSPARC_EIO, "index lines of indices.txt differ in length");
+    // values
+    float *val = (float *)std::malloc(sizeof(float) * std::max<uint64_t>(nnz, 1));
+    uint64_t *idx = (uint64_t *)std::malloc(sizeof(uint64_t) * std::max<uint64_t>((uint64_t)order * nnz, 1));
+    if (!val || !idx) {
+        std::free(val);
+        std::free(idx);
+        fail(GSPARC_ENOMEM, "host allocation failed");
+    }
+    {
+        const char *p = vb.data();
+        for (uint64_t k = 0; k < nnz; ++k) {
+            while (*p && (is_sep(*p) || *p == '\n')) ++p;
+            char *end = nullptr;
+            const double v = *p ? std::strtod(p, &end) : 0.0;
+            if (!*p || end == p) {
+                std::free(val);
+                std::free(idx);
+                fail(GSPARC_EIO, "values.txt holds fewer values than there are nonzeros");
+            }
+            val[k] = (float)v;
+            p = end;
+        }
+    }
+    for (int m = 0; m < order; ++m) {
+        uint64_t mx = 0;
+        for (uint64_t k = 0; k < nnz; ++k) {
+            idx[(uint64_t)m * nnz + k] = rows[m][k];
+            mx = std::max(mx, rows[m][k] + 1);
+        }
+        dims_out[m] = mx;
+    }
+    *order_out = order;
+    *nnz_out = nnz;
+    *idx_out = idx;
+    *val_out = val;
+}
+
 void write_tns(const char *path, int order, uint64_t nnz, const uint64_t *idx, const float *val) {
     FILE *f = std::fopen(path, "w");
     if (!f) fail(GSPARC_EIO, std::string("cannot open ") + path + " for writing");

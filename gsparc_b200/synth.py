@@ -277,6 +277,18 @@ def write_tns(path: str, t: CooTensor) -> None:
             f.write("\n")
 
 
+def write_quantum(path: str, t: CooTensor) -> None:
+    """Write the quantum-chemistry directory format: ``path/indices.txt``, one
+    line of 1-based indices per mode, and ``path/values.txt``, one value per
+    line (``%.9g``)."""
+    os.makedirs(path, exist_ok=True)
+    with open(os.path.join(path, "indices.txt"), "w") as f:
+        for m in range(t.order):
+            f.write(" ".join(np.char.mod("%d", (t.idx[m] + np.uint64(1)).astype(np.int64))) + "\n")
+    with open(os.path.join(path, "values.txt"), "w") as f:
+        f.write("\n".join(np.char.mod("%.9g", t.val.astype(np.float64))) + "\n")
+
+
 def read_tns_py(path: str) -> CooTensor:
     """Small pure-Python reader with the reference's dims rule (test helper)."""
     rows = []

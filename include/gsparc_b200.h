@@ -138,6 +138,10 @@ gsparc_status gsparc_tensor_upload(gsparc_ctx *ctx, const gsparc_coo *coo, void 
 gsparc_status gsparc_tensor_free(gsparc_ctx *ctx, gsparc_tensor *t);
 gsparc_status gsparc_tensor_info(const gsparc_tensor *t, int *order, uint64_t *dims /*[32]*/,
                                  uint64_t *nnz);
+/* Copy a resident tensor to host memory: idx SoA (idx[m*nnz + k], order*nnz
+ * entries), val nnz entries.  The reference copies its result keys to the
+ * host the same way (include/gsparc/contraction.cuh:554-561). */
+gsparc_status gsparc_tensor_download(const gsparc_tensor *t, uint64_t *idx, float *val, void *stream);
 
 /* ---- the contraction ------------------------------------------------------ */
 /* Z = X x_{cx,cy} Y.  Replaces gsparc::SpTC (include/gsparc/sptc.cuh:16-360)
@@ -158,6 +162,18 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
                                 int ncmodes, const int *cx, const int *cy, int accum,
                                 int shard, int nshards,
                                 const gsparc_sink *sink, gsparc_stats *stats, void *stream);
+
+/* Z = X x_{cx,cy} Y kept on the device as a resident COO tensor: its modes
+ * are X's free modes (ascending) followed by Y's free modes (ascending), and
+ * it can be an operand of any later contraction (free it with
+ * gsparc_tensor_free).  Replaces the reference's multi-SpTC chaining
+ * (main.cu:323-371, include/gsparc/sptc.cuh:362-698), which keeps the first
+ * result's keys and reuses them as the next contraction's X keys.  Z must fit
+ * the context's budget (12 B per output nonzero while collecting, then
+ * 8 B per mode + 4 B per nonzero). */
+gsparc_status gsparc_sptc_resident(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y,
+                                   int ncmodes, const int *cx, const int *cy, int accum,
+                                   gsparc_tensor **Z, gsparc_stats *stats, void *stream);
 
 /* One contraction of a batch: the arguments of gsparc_sptc plus per-job
  * results. */
@@ -264,6 +280,12 @@ gsparc_status gsparc_serve_reset_stats(gsparc_server *srv);
  * library (free with gsparc_free_host); idx is SoA: idx[m*nnz + k]. */
 gsparc_status gsparc_read_tns(const char *path, int nthreads, int *order, uint64_t *dims /*[32]*/,
                               uint64_t *nnz, uint64_t **idx, float **val);
+/* Parse the quantum-chemistry directory format (the reference's -q):
+ * <dir>/indices.txt holds one line per mode with the 1-based indices of all
+ * nonzeros, <dir>/values.txt the values.  Replaces IOManager::_ReadQuantumData
+ * (include/gsparc/io_manager.tpp:310-484).  Output arrays as gsparc_read_tns. */
+gsparc_status gsparc_read_quantum(const char *dir, int nthreads, int *order, uint64_t *dims /*[32]*/,
+                                  uint64_t *nnz, uint64_t **idx, float **val);
 /* Write 1-based text COO with %.9g values. */
 gsparc_status gsparc_write_tns(const char *path, int order, uint64_t nnz,
                                const uint64_t *idx /* SoA idx[m*nnz+k] */, const float *val);

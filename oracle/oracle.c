@@ -18,6 +18,7 @@
  *   index match         include/gsparc/indexMatch.cuh:20-44,67-118,231-287
  *   ESC expand          include/gsparc/contraction.cuh:100-141 (key x_f<<Y_nfbits | y_f)
  *   sort + reduce       include/gsparc/contraction.cuh:506-537 (ascending keys, Sum)
+ *   quantum input       include/gsparc/io_manager.tpp:310-484 (indices.txt + values.txt)
  *   keys over 64 bits   include/gsparc/tensor_manager.tpp:301-406 (ConvertTensor_extra:
  *                       the same layouts in a 128-bit key), include/gsparc/indexMatch.cuh:
  *                       120-229 (match on the full 128-bit contract key); output keys
@@ -610,6 +611,143 @@ int oracle_read_tns(const char *path, int *order_out, uint64_t *nnz_out,
     free(buf);
     *order_out = order;
     *nnz_out = n;
+    *idx_out = idx;
+    *val_out = val;
+    return OR_OK;
+}
+
+/*
+ * io_manager.tpp:310-484 (_ReadQuantumData, read_txt_dims_parallel,
+ * read_txt_data_parallel): <dir>/indices.txt holds one line per mode, each
+ * with the 1-based index of every nonzero (parsed with strtod); order = number
+ * of lines, nnz = tokens per line, dims[m] = largest index of mode m;
+ * <dir>/values.txt holds nnz values.  Values are read as double and narrowed
+ * to float (the reference scans "%le" into its float array, which this
+ * restatement does not copy).  Lines without a token are skipped.
+ */
+static char *slurp_text(const char *path)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f)
+        return NULL;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    rewind(f);
+    char *b = (char *)malloc((size_t)(sz > 0 ? sz : 0) + 1);
+    if (!b) {
+        fclose(f);
+        return NULL;
+    }
+    size_t r = sz > 0 ? fread(b, 1, (size_t)sz, f) : 0;
+    fclose(f);
+    b[r] = '\0';
+    return b;
+}
+
+int oracle_read_quantum(const char *dir, int *order_out, uint64_t *nnz_out,
+                        uint64_t *dims_out /* [64] */, uint64_t **idx_out, float **val_out)
+{
+    char path[4096];
+    snprintf(path, sizeof path, "%s/indices.txt", dir);
+    char *ib = slurp_text(path);
+    snprintf(path, sizeof path, "%s/values.txt", dir);
+    char *vb = slurp_text(path);
+    if (!ib || !vb) {
+        free(ib);
+        free(vb);
+        return OR_EIO;
+    }
+    /* pass 1: order and nnz (tokens of each non-empty line) */
+    int order = 0;
+    uint64_t nnz = 0;
+    int bad = 0;
+    for (char *p = ib; *p;) {
+        char *e = strchr(p, '\n');
+        char *end = e ? e : p + strlen(p);
+        uint64_t cnt = 0;
+        char *q = p;
+        while (q < end) {
+            while (q < end && (*q == ' ' || *q == '\t' || *q == '\r'))
+                ++q;
+            if (q >= end)
+                break;
+            ++cnt;
+            while (q < end && !(*q == ' ' || *q == '\t' || *q == '\r'))
+                ++q;
+        }
+        if (cnt) {
+            if (order == 0)
+                nnz = cnt;
+            else if (cnt != nnz)
+                bad = 1;
+            ++order;
+        }
+        p = e ? e + 1 : end;
+    }
+    if (bad || order == 0 || order > 64) {
+        free(ib);
+        free(vb);
+        return OR_EIO;
+    }
+    uint64_t *idx = (uint64_t *)malloc(8 * (size_t)order * (nnz ? nnz : 1));
+    float *val = (float *)malloc(4 * (nnz ? nnz : 1));
+    if (!idx || !val) {
+        free(ib);
+        free(vb);
+        free(idx);
+        free(val);
+        return OR_ENOMEM;
+    }
+    /* pass 2: indices, row by row */
+    int m = 0;
+    for (char *p = ib; *p && m < order;) {
+        char *e = strchr(p, '\n');
+        if (e)
+            *e = '\0';
+        uint64_t k = 0, mx = 0;
+        char *q = p;
+        for (;;) {
+            char *end;
+            double v = strtod(q, &end);
+            if (end == q)
+                break;
+            if (!(v >= 1.0) || v != (double)(uint64_t)v)
+                bad = 1;
+            uint64_t i0 = (uint64_t)v - 1;
+            if (k < nnz)
+                idx[(uint64_t)m * nnz + k] = i0;
+            if (i0 + 1 > mx)
+                mx = i0 + 1;
+            ++k;
+            q = end;
+        }
+        if (k) {
+            dims_out[m] = mx;
+            ++m;
+        }
+        p = e ? e + 1 : p + strlen(p);
+    }
+    /* values */
+    char *q = vb;
+    for (uint64_t k = 0; k < nnz; ++k) {
+        char *end;
+        double v = strtod(q, &end);
+        if (end == q) {
+            bad = 1;
+            break;
+        }
+        val[k] = (float)v;
+        q = end;
+    }
+    free(ib);
+    free(vb);
+    if (bad) {
+        free(idx);
+        free(val);
+        return OR_EIO;
+    }
+    *order_out = order;
+    *nnz_out = nnz;
     *idx_out = idx;
     *val_out = val;
     return OR_OK;

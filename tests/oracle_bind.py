@@ -60,6 +60,7 @@ def lib():
                                   ctypes.POINTER(ctypes.POINTER(_Result))]
         L.oracle_free.argtypes = [ctypes.POINTER(_Result)]
         L.oracle_read_tns.argtypes = [ctypes.c_char_p, P, P, P, P, P]
+        L.oracle_read_quantum.argtypes = [ctypes.c_char_p, P, P, P, P, P]
         L.oracle_free_buf.argtypes = [P]
         _lib = L
     return _lib
@@ -161,16 +162,23 @@ def sptc(X, Y, cx, cy, max_products: int = 200_000_000) -> OracleZ:
 
 
 def read_tns(path: str):
+    return _read(lib().oracle_read_tns, path)
+
+
+def read_quantum(path: str):
+    return _read(lib().oracle_read_quantum, path)
+
+
+def _read(fn, path: str):
     from gsparc_b200.synth import CooTensor
     order = np.zeros(1, np.int32)
     nnz = np.zeros(1, np.uint64)
     dims = np.zeros(64, np.uint64)
     pidx = ctypes.c_void_p()
     pval = ctypes.c_void_p()
-    st = lib().oracle_read_tns(path.encode(), _p(order), _p(nnz), _p(dims),
-                               ctypes.byref(pidx), ctypes.byref(pval))
+    st = fn(path.encode(), _p(order), _p(nnz), _p(dims), ctypes.byref(pidx), ctypes.byref(pval))
     if st:
-        raise ValueError(f"oracle_read_tns status {st}")
+        raise ValueError(f"oracle read status {st}")
     o = int(order[0]); n = int(nnz[0])
     idx = np.ctypeslib.as_array(ctypes.cast(pidx, ctypes.POINTER(ctypes.c_uint64)),
                                 shape=(o * max(n, 1),))[: o * n].reshape(o, n).copy()

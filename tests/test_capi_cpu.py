@@ -147,9 +147,19 @@ def test_context_without_gpu_returns_status_not_crash():
 def test_cli_rejects_unsupported_and_bad_arguments(tmp_path):
     cli = gb.CLI_PATH
     assert os.path.exists(cli)
-    r = subprocess.run([cli, "-X", "a", "-Y", "b", "-c", "1", "-x", "0", "-y", "0", "-q"],
+    r = subprocess.run([cli, "-X", "/none/qa", "-Y", "/none/qb", "-c", "1", "-x", "0", "-y", "0", "-q"],
                        capture_output=True, text=True)
-    assert r.returncode == 1 and "quantum" in r.stderr
+    assert r.returncode == 1 and "indices.txt" in r.stderr
+    # chained multi-SpTC runs on one GPU and needs -a/-z consistent with Y
+    d = tmp_path
+    synth.write_tns(str(d / "a.tns"), synth.make_tensor([5, 6, 7], 20, ["uniform"] * 3, "u01", 1))
+    r = subprocess.run([cli, "-X", str(d / "a.tns"), "-Y", str(d / "a.tns"), "-c", "1", "-x", "2", "-y", "2",
+                        "-m", "1", "-a", "1", "-z", "0", "-g", "2"], capture_output=True, text=True)
+    assert r.returncode == 1 and "one GPU" in r.stderr
+    assert "multi_sptc: 1" in r.stderr and "# contract modes of Z (second SpTC): 1, contract modes: 0 \n" in r.stderr
+    r = subprocess.run([cli, "-X", str(d / "a.tns"), "-Y", str(d / "a.tns"), "-c", "1", "-x", "2", "-y", "2",
+                        "-m", "1", "-a", "3", "-z", "0", "1", "2"], capture_output=True, text=True)
+    assert r.returncode == 1 and "-a N" in r.stderr
     r = subprocess.run([cli, "-X", "a"], capture_output=True, text=True)
     assert r.returncode == 1 and "Usage" in r.stderr
     r = subprocess.run([cli, "-X", "/none/a.tns", "-Y", "/none/b.tns", "-c", "2", "-x", "0", "1",
@@ -160,3 +170,55 @@ def test_cli_rejects_unsupported_and_bad_arguments(tmp_path):
     assert "# contract modes of X: 2, contract modes: 0 1 \n" in r.stderr
     assert "# contract modes of Y: 2, contract modes: 1 0 \n" in r.stderr
     assert "dense_accumulator: -1" in r.stderr
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_read_quantum_matches_oracle_parser(tmp_path, seed):
+    t = synth.make_tensor([30, 7, 120, 9], 400, ["uniform", ("zipf", 1.2), "uniform", "uniform"], "normal", seed)
+    d = str(tmp_path / "q")
+    synth.write_quantum(d, t)
+    a = gb.read_quantum(d)
+    b = ob.read_quantum(d)
+    assert a.dims == b.dims == t.dims
+    assert np.array_equal(a.idx, b.idx) and np.array_equal(a.idx, t.idx)
+    assert np.array_equal(a.val, b.val) and np.array_equal(a.val, t.val)
+    # the same tensor through .tns reads identically
+    p = str(tmp_path / "t.tns")
+    synth.write_tns(p, t)
+    c = gb.read_tns(p)
+    assert c.dims == a.dims and np.array_equal(c.idx, a.idx) and np.array_equal(c.val, a.val)
+
+
+def test_read_quantum_number_formats_and_blank_lines(tmp_path):
+    d = tmp_path / "q"
+    d.mkdir()
+    (d / "indices.txt").write_text("1 3.0\t2\n\n4 4 1\r\n")
+    (d / "values.txt").write_text("1.5e0\n-2.25\n\n3E-1\n")
+    a = gb.read_quantum(str(d))
+    b = ob.read_quantum(str(d))
+    assert a.dims == b.dims == [3, 4]
+    assert a.idx.tolist() == b.idx.tolist() == [[0, 2, 1], [3, 3, 0]]
+    assert a.val.tolist() == b.val.tolist() == [1.5, -2.25, np.float32(0.3)]
+
+
+@pytest.mark.parametrize("idx,vals", [("1 2\n1\n", "1 2\n"),        # lines of different lengths
+                                      ("1 0\n1 1\n", "1 2\n"),      # index 0 (indices are 1-based)
+                                      ("1 2.5\n1 1\n", "1 2\n"),    # non-integral index
+                                      ("1 2\n1 1\n", "1\n"),         # fewer values than nonzeros
+                                      ("", "")])                         # no modes
+def test_read_quantum_reports_malformed_input(tmp_path, idx, vals):
+    d = tmp_path / "q"
+    d.mkdir()
+    (d / "indices.txt").write_text(idx)
+    (d / "values.txt").write_text(vals)
+    with pytest.raises(gb.GsparcError) as e:
+        gb.read_quantum(str(d))
+    assert e.value.status == 4
+    with pytest.raises(ValueError):
+        ob.read_quantum(str(d))
+
+
+def test_read_quantum_missing_directory():
+    with pytest.raises(gb.GsparcError) as e:
+        gb.read_quantum("/none/such/dir")
+    assert e.value.status == 4
