@@ -152,7 +152,7 @@ def run_sparta(xs_path, y_path, threads, timeout=600):
         return None
     env = dict(os.environ, EXPERIMENT_MODES="3")
     cmd = [ttt, "-X", xs_path, "-Y", y_path, "-m", "2", "-x", "2", "3", "-y", "2", "3", "-t", str(threads)]
-    for _ in range(3):  # the baseline binary is not robust on every run; retry
+    for _ in range(10):  # the baseline binary crashes on about half of its runs here; retry
         try:
             r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=timeout)
         except subprocess.TimeoutExpired:
@@ -525,6 +525,7 @@ def ours_arm(args, world, rank, local, dist):
             "heavy_windows": s0["heavy_windows"], "heavy_rows": s0["heavy_rows"], "rows": s0["rows"],
             "stage_ms": {k: s0[k] for k in ("t_linearize_ms", "t_sort_ms", "t_match_ms", "t_plan_ms",
                                              "t_contract_ms", "t_total_ms")},
+            "step_total_ms": [round(s["t_total_ms"], 3) for s in stats],
         }
         print(json.dumps(line), flush=True)
 

@@ -150,12 +150,14 @@ __device__ __forceinline__ uint32_t compact_parts(uint32_t nb, uint32_t *seg_sta
 }
 
 // Flattened walk over the non-empty parts seg[0..ns): every entry idx of every
-// part is visited once, entries spread evenly over the CTA's warps.  Each warp
-// step takes ILP chunks of 32 consecutive entries; load(k, idx, item) runs for
-// all of them before body(k, idx, item) runs for any, so a warp keeps ILP
-// independent memory loads in flight.  Lanes find their part with a shuffle
-// search over the next 32 part boundaries (parts are non-empty, so at most 32
-// of them start inside a chunk of 32 entries).
+// part is visited once, entries spread evenly over the CTA's warps.  Warp w
+// owns one contiguous stretch of the flattened index space; its lanes step
+// through it 32 entries apart (coalesced loads), ILP steps at a time, so load
+// runs for ILP entries before body runs for any of them and a warp keeps ILP
+// independent memory loads in flight.  A lane finds the part of its first
+// entry by binary search over the part offsets and then only moves forward:
+// it advances to the next part whenever its entry passes the current part's
+// end, so mapping an entry to (part, index) costs a compare and an add.
 constexpr int ILP = 4;
 
 template <class Item, class Load, class Body>
@@ -163,36 +165,40 @@ __device__ __forceinline__ void flat_for(const uint32_t *seg_start, const uint32
                                          Load &&load, Body &&body) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tot = seg_off[ns];
-    uint32_t k = 0;  // warp-uniform: the part holding the chunk's first entry
-    for (uint32_t base = warp * 32u * ILP; base < tot; base += NWARPS * 32u * ILP) {
+    constexpr uint32_t STEP = 32u * ILP;
+    const uint32_t steps = (tot + STEP - 1) / STEP;       // warp steps in all
+    const uint32_t per_warp = (steps + NWARPS - 1) / NWARPS;
+    const uint32_t t0 = warp * per_warp * STEP + lane;    // this lane's first entry
+    const uint32_t tend = min(tot, (warp + 1) * per_warp * STEP);
+    if (t0 >= tend) return;
+    // part holding t0: the last k with seg_off[k] <= t0 (seg_off[0] = 0, seg_off[ns] = tot > t0)
+    uint32_t lo = 0, hi = ns;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (seg_off[mid] <= t0)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    uint32_t k = lo;
+    uint32_t next = seg_off[k + 1];         // end of part k in the flattened space
+    uint32_t base = seg_start[k] - seg_off[k];  // idx = base + t inside part k (mod 2^32)
+    for (uint32_t t = t0; t < tend; t += STEP) {
         uint32_t kk[ILP], idx[ILP];
         bool ok[ILP];
 #pragma unroll
         for (int u = 0; u < ILP; ++u) {
-            const uint32_t cb = base + 32u * u;
-            // seg_off is increasing, so "seg_off[j] <= cb" holds for a prefix of j
-            for (;;) {
-                const uint32_t j = k + 1 + lane;
-                const bool le = j < ns && seg_off[j] <= cb;
-                const uint32_t n = __popc(__ballot_sync(FULL, le));
-                k += n;
-                if (n < 32) break;
+            const uint32_t tu = t + 32u * u;
+            ok[u] = tu < tend;
+            if (ok[u]) {
+                while (tu >= next) {  // parts are non-empty and k + 1 < ns while tu < tot
+                    ++k;
+                    next = seg_off[k + 1];
+                    base = seg_start[k] - seg_off[k];
+                }
             }
-            const uint32_t t = cb + lane;
-            const uint32_t bj = (k + 1 + lane <= ns) ? seg_off[k + 1 + lane] : INF;
-            // c = number of part boundaries in (cb, t]; every part holds at least
-            // one entry, so at most 31 of them fall inside the chunk and the
-            // 5-step lifting over the 32 loaded boundaries is exact
-            uint32_t c = 0;
-#pragma unroll
-            for (uint32_t step = 16; step >= 1; step >>= 1) {
-                const uint32_t b = __shfl_sync(FULL, bj, c + step - 1);
-                if (b <= t) c += step;
-            }
-            const uint32_t q = k + c;
-            ok[u] = t < tot && q < ns;  // q < ns always holds when t < tot; checked, not trusted
-            kk[u] = q;
-            idx[u] = ok[u] ? seg_start[q] + (t - seg_off[q]) : 0u;
+            kk[u] = k;
+            idx[u] = base + tu;
         }
         Item it[ILP];
 #pragma unroll
