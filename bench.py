@@ -40,7 +40,9 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "esc_large"
 METRIC = "matched products/sec"
 UNIT = "products/s"
-TRAFFIC_BYTES_PER_OUTPUT = 2.789e9 / 2.3186e8  # ncu DRAM bytes / outputs, numeric pass, scale 0.1
+# ncu DRAM bytes (read + write) of the numeric launches (k_light<1>, k_rowwin<1>, k_stream) per output
+# nonzero, measured on esc_large at scale 0.1 (one output chunk, 2.50e8 outputs)
+TRAFFIC_BYTES_PER_OUTPUT = (27.8e6 + 2849.5e6) / 2.50473870e8
 
 
 def parse():
@@ -436,10 +438,10 @@ def ours_arm(args, world, rank, local, dist):
     alg_bytes = 12.0 * s0["nnz"] + 16.0 * s0["nnz_x"] + 8.0 * s0["nnz_y"]
     peaks = load_peaks()
     achieved = alg_bytes / (t_num / 1e3) / 1e9
-    # DRAM traffic of the numeric pass measured with ncu at scale 0.1 (profiles/k_rowwin_esc_large.md):
-    # 2.789 GB written for 2.32e8 heavy-row outputs, reads < 1%; it scales with the outputs.
+    # DRAM traffic of the numeric pass measured with ncu at scale 0.1: 11.5 B per output nonzero,
+    # almost all of it the output writes; it scales with the outputs.
     traffic = TRAFFIC_BYTES_PER_OUTPUT * s0["nnz"] / max(1, s0["chunks"])
-    roofline = {"bound": "hbm", "kernel": "k_rowwin<numeric> + k_light<numeric>",
+    roofline = {"bound": "hbm", "kernel": "k_rowwin<numeric> + k_light<numeric> + k_stream",
                 "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                 "traffic": traffic, "traffic_scope": "per numeric launch (one per output chunk), "
