@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work per baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-stream (batched / served) lines")
-    ap.add_argument("--mixed-count", type=int, default=256, help="instances of the mixed stream")
+    ap.add_argument("--mixed-count", type=int, default=256, help="instances of the batched / served streams")
     return ap.parse_args()
 
 
@@ -171,7 +171,8 @@ class CpuBaseline:
     def __init__(self, X, target_seconds: float):
         import gsparc_b200 as gb
         self.X = X
-        self.threads = os.cpu_count() or 1
+        # the cores this process may run on (the host may have more than the job is given)
+        self.threads = len(os.sched_getaffinity(0)) or 1
         self.dir = tempfile.mkdtemp(prefix="gsparc_cpu_")
         self.y_path = os.path.join(self.dir, "y.tns")
         gb.write_tns(self.y_path, X.idx, X.val)
@@ -216,14 +217,17 @@ class CpuBaseline:
                              if self.kind == "reference" else "CPU oracle (ESC, FP64), wall time")}
 
 
-def mixed_stream(args, device, sp, stream):
-    """The mixed stream of independent contractions (orders 3-4, modes
-    log-uniform 64..100k, nnz log-uniform 1e3..1e6, 1-2 contract modes,
-    Zipf s in [1.0,1.4], U[-1,1), seed 3), run three ways on the same
-    resident operands: plain (one gsparc_sptc per contraction, in order),
-    batched (one gsparc_sptc_batch) and served (Poisson arrivals at a mean
-    2000 requests/s into a gsparc_serve_* server; the plain form answers the
-    same arrivals one at a time)."""
+def pct(v, p):
+    """Nearest-rank percentile of sorted values."""
+    return float(v[max(1, int(math.ceil(p / 100.0 * len(v)))) - 1])
+
+
+def batched_stream(args, device, sp, stream):
+    """The batched workload (256 independent contractions: orders 3-4, modes
+    log-uniform 64..100k, nnz log-uniform 1e3..1e6, 1-2 contract modes, Zipf
+    s in [1.0,1.4], U[-1,1), seed 3) run two ways on the same resident
+    operands: plain (one gsparc_sptc per contraction, in order) and batched
+    (one gsparc_sptc_batch)."""
     import torch
     import gsparc_b200 as gb
     from gsparc_b200 import synth
@@ -256,26 +260,39 @@ def mixed_stream(args, device, sp, stream):
     torch.cuda.synchronize()
     batched_ms = e0.elapsed_time(e1)
     assert bst["ir_nnz"] == ir
-
     for dx, dy in ops:
         dx.free()
         dy.free()
-    ctx.close()  # the server gets the device's memory to itself
+    ctx.close()
+    desc = (f"{len(jobs)} independent contractions, {nnz} operand nonzeros, {ir:.4e} matched products "
+            "(orders 3-4, modes log-uniform 64..100k, nnz log-uniform 1e3..1e6, 1-2 contract modes, "
+            "Zipf s 1.0-1.4, U[-1,1), seed 3)")
+    return {"workload": desc, "unit": UNIT,
+            "plain_value": ir / (plain_ms / 1e3), "plain_ms": plain_ms,
+            "batched_value": ir / (batched_ms / 1e3), "batched_ms": batched_ms,
+            "batched_over_plain": plain_ms / batched_ms, "groups_launches": bst["kernel_launches"],
+            "timing": "CUDA events on the launching stream, each form after one warm-up pass"}
 
-    # served: the same contractions arriving as a Poisson stream
-    rng = np.random.default_rng(17)
-    arrive = np.cumsum(rng.exponential(1.0 / 2000.0, size=len(jobs)))
+
+def served_stream(args, device, sp, stream):
+    """The served workload, bounded so a run stays within minutes: 256 requests
+    with operand orders 3-5, 1-2 contract modes, modes log-uniform 64..100k,
+    operand nnz from a power law n^-1.5 on [1e4, 2e6], Zipf s in [1.0,1.4]
+    indices, U[-1,1) values, Poisson arrivals at a mean 2000/s (seed 5), into
+    a gsparc_serve_* server with a 150 GB budget (less if the GPU has less
+    free); the plain form answers the same arrivals one at a time."""
+    import torch
+    import gsparc_b200 as gb
+    from gsparc_b200 import synth
+    inst, arrive = synth.served_stream(args.mixed_count, seed=5, max_nnz=2_000_000)
+    nnz = sum(X.nnz + Y.nnz for X, Y, _, _ in inst)
     free_b, _ = torch.cuda.mem_get_info()
-    budget = min(150 << 30, int(free_b * 0.9))
+    budget = min(150 << 30, int(free_b * 0.8))
 
     def served_run(lanes):
         srv = gb.Server(device, hbm_budget=budget, lanes=lanes)
         sops = [(srv.upload(X), srv.upload(Y)) for X, Y, _, _ in inst]
-        # warm-up: the whole stream once, unpaced (as the other forms get one pass)
-        for t in [srv.submit(sx, sy, cx, cy, sink="discard") for (sx, sy), (_, _, cx, cy) in zip(sops, inst)]:
-            srv.wait(t)
-        srv.reset_stats()
-        tickets = [None] * len(jobs)
+        tickets = [None] * len(inst)
 
         def client():
             t0 = time.perf_counter()
@@ -284,11 +301,16 @@ def mixed_stream(args, device, sp, stream):
                 if d > 0:
                     time.sleep(d)
                 tickets[i] = srv.submit(sx, sy, cx, cy, sink="discard")
-        th = threading.Thread(target=client)
-        th.start()
-        th.join()
-        for t in tickets:
-            srv.wait(t)
+        # one untimed pass of the same paced stream (the server's memory pool
+        # grows to its working size there, as the plain form gets a warm-up
+        # pass), then the timed one
+        for rep in range(2):
+            srv.reset_stats()
+            th = threading.Thread(target=client)
+            th.start()
+            th.join()
+            for t in tickets:
+                srv.wait(t)
         st = srv.stats()
         srv.close()
         return st
@@ -296,10 +318,10 @@ def mixed_stream(args, device, sp, stream):
     sst1 = served_run(1)
 
     # plain form on the same arrivals: one contraction at a time, in order
-    ctx = gb.Context(device)
+    ctx = gb.Context(device, hbm_budget=budget)
     ops = [(ctx.upload(X, stream=sp), ctx.upload(Y, stream=sp)) for X, Y, _, _ in inst]
     jobs = [(dx, dy, cx, cy) for (dx, dy), (_, _, cx, cy) in zip(ops, inst)]
-    plain_once()
+    ir = sum(gb.sptc(ctx, dx, dy, cx, cy, 0, sink="discard", stream=sp).ir_nnz for dx, dy, cx, cy in jobs)
     torch.cuda.synchronize()
     lat = []
     t0 = time.perf_counter()
@@ -311,34 +333,28 @@ def mixed_stream(args, device, sp, stream):
         lat.append((time.perf_counter() - t0 - arrive[i]) * 1e3)
     plain_wall = time.perf_counter() - t0
     lat = np.sort(np.asarray(lat))
-
-    def pct(v, p):
-        return float(v[max(1, int(math.ceil(p / 100.0 * len(v)))) - 1])
     for dx, dy in ops:
         dx.free()
         dy.free()
     ctx.close()
-    desc = (f"{len(jobs)} independent contractions, {nnz} operand nonzeros, {ir:.4e} matched products "
-            "(orders 3-4, modes log-uniform 64..100k, nnz log-uniform 1e3..1e6, 1-2 contract modes, "
-            "Zipf s 1.0-1.4, U[-1,1), seed 3)")
-    batched = {"workload": desc, "unit": UNIT,
-               "plain_value": ir / (plain_ms / 1e3), "plain_ms": plain_ms,
-               "batched_value": ir / (batched_ms / 1e3), "batched_ms": batched_ms,
-               "batched_over_plain": plain_ms / batched_ms, "groups_launches": bst["kernel_launches"],
-               "timing": "CUDA events on the launching stream, each form after one warm-up pass"}
-    served = {"workload": desc + f"; Poisson arrivals, mean 2000/s, seed 17; HBM budget {budget / 2**30:.0f} GiB",
-              "unit": UNIT, "value": sst["products_per_s"], "p50_ms": sst["p50_ms"], "p99_ms": sst["p99_ms"],
-              "mean_ms": sst["mean_ms"], "wall_ms": sst["wall_ms"], "batches": sst["batches"],
-              "max_batch": sst["max_batch"], "max_in_flight": sst["max_in_flight"],
-              "plain_value": ir / plain_wall, "plain_p50_ms": pct(lat, 50), "plain_p99_ms": pct(lat, 99),
-              "plain_wall_ms": plain_wall * 1e3, "served_over_plain": sst["products_per_s"] / (ir / plain_wall),
-              "lanes": 2,
-              "one_lane": {"value": sst1["products_per_s"], "p50_ms": sst1["p50_ms"], "p99_ms": sst1["p99_ms"],
-                           "wall_ms": sst1["wall_ms"], "batches": sst1["batches"],
-                           "served_over_plain": sst1["products_per_s"] / (ir / plain_wall)},
-              "timing": "host clock: latency = submission to result delivered; the plain form runs "
-                        "each request when it has arrived and the previous one finished"}
-    return batched, served
+    assert sst["ir_nnz"] == ir
+    wide = sum(1 for X, Y, _, _ in inst
+               if sum(synth._bits(d) for d in X.dims) > 64 or sum(synth._bits(d) for d in Y.dims) > 64)
+    desc = (f"{len(inst)} requests, {nnz} operand nonzeros, {ir:.4e} matched products (operand orders 3-5, "
+            "1-2 contract modes, modes log-uniform 64..100k, nnz power law n^-1.5 on [1e4, 2e6], Zipf s 1.0-1.4, "
+            f"U[-1,1), {wide} with operand keys over 64 bits, seed 5); Poisson arrivals, mean 2000/s; "
+            f"HBM budget {budget / 2**30:.0f} GiB")
+    return {"workload": desc, "unit": UNIT, "value": sst["products_per_s"], "p50_ms": sst["p50_ms"],
+            "p99_ms": sst["p99_ms"], "mean_ms": sst["mean_ms"], "wall_ms": sst["wall_ms"],
+            "batches": sst["batches"], "max_batch": sst["max_batch"], "max_in_flight": sst["max_in_flight"],
+            "plain_value": ir / plain_wall, "plain_p50_ms": pct(lat, 50), "plain_p99_ms": pct(lat, 99),
+            "plain_wall_ms": plain_wall * 1e3, "served_over_plain": sst["products_per_s"] / (ir / plain_wall),
+            "lanes": 2,
+            "one_lane": {"value": sst1["products_per_s"], "p50_ms": sst1["p50_ms"], "p99_ms": sst1["p99_ms"],
+                         "wall_ms": sst1["wall_ms"], "batches": sst1["batches"],
+                         "served_over_plain": sst1["products_per_s"] / (ir / plain_wall)},
+            "timing": "host clock: latency = submission to result delivered; the plain form runs "
+                      "each request when it has arrived and the previous one finished"}
 
 
 # --------------------------------------------------------------------------- arms
@@ -499,7 +515,8 @@ def ours_arm(args, world, rank, local, dist):
     ctx.close()  # returns the large workload's memory before the mixed stream
     batched = served = None
     if world == 1 and not args.no_mixed:
-        batched, served = mixed_stream(args, local, sp, stream)
+        batched = batched_stream(args, local, sp, stream)
+        served = served_stream(args, local, sp, stream)
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:

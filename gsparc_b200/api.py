@@ -109,7 +109,8 @@ class ServeStats(ctypes.Structure):
                 ("nnz", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
                 ("products_per_s", ctypes.c_double), ("resident_bytes", ctypes.c_uint64),
-                ("peak_reserved_bytes", ctypes.c_uint64), ("max_in_flight", ctypes.c_uint64)]
+                ("peak_reserved_bytes", ctypes.c_uint64), ("max_in_flight", ctypes.c_uint64),
+                ("retries", ctypes.c_uint64), ("chunks", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -97,7 +97,7 @@ struct gsparc_server {
     // statistics
     std::vector<double> lat_ms;
     uint64_t submitted = 0, completed = 0, failed = 0, batches = 0, max_batch = 0;
-    uint64_t ir = 0, nnz = 0, peak_reserved = 0, max_in_flight = 0;
+    uint64_t ir = 0, nnz = 0, peak_reserved = 0, max_in_flight = 0, retries = 0, chunks = 0;
     Clock::time_point t_first, t_last;
     bool have_first = false;
 
@@ -185,15 +185,23 @@ void run_batch(gsparc_server *S, Lane *L, std::vector<Req *> &batch, uint64_t re
     if (jobs.size() > 1) {
         for (size_t i = 0; i < jobs.size(); ++i) {
             if (fin[i] || jobs[i].status != GSPARC_ENOMEM) continue;
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                S->retries += 1;
+            }
             jobs[i] = batch[i]->job;
             try {
-                gs::sptc_batch(&L->ctx, &jobs[i], 1, S->opt.max_chunk_nnz, &bst, L->stream);
+                gsparc_stats rst;
+                std::memset(&rst, 0, sizeof(rst));
+                gs::sptc_batch(&L->ctx, &jobs[i], 1, S->opt.max_chunk_nnz, &rst, L->stream);
+                bst.chunks += rst.chunks;
             } catch (...) {
             }
             cudaStreamSynchronize(L->stream);
         }
     }
     std::lock_guard<std::mutex> lk(S->mu);
+    S->chunks += bst.chunks;
     for (size_t i = 0; i < batch.size(); ++i)
         if (!fin[i]) complete_locked(S, batch[i], jobs[i]);
 }
@@ -533,6 +541,8 @@ gsparc_status gsparc_serve_stats(gsparc_server *srv, gsparc_server_stats *out) {
         out->resident_bytes = srv->resident.in_use();
         out->peak_reserved_bytes = srv->peak_reserved;
         out->max_in_flight = srv->max_in_flight;
+        out->retries = srv->retries;
+        out->chunks = srv->chunks;
         std::vector<double> v = srv->lat_ms;
         if (!v.empty()) {
             std::sort(v.begin(), v.end());
@@ -565,6 +575,7 @@ gsparc_status gsparc_serve_reset_stats(gsparc_server *srv) {
         srv->ir = srv->nnz = 0;
         srv->peak_reserved = srv->reserved;
         srv->max_in_flight = srv->running;
+        srv->retries = srv->chunks = 0;
         srv->have_first = false;
     });
 }

@@ -12,7 +12,8 @@ engine is measured on:
 * ``dense_acc``     X 200x4096x4096 and Y 4096x4096x300, 10M nnz each,
   contract modes Zipf(s=1.2), free modes uniform, N(0,1)
   (``-c 2 -x 1 2 -y 0 1``).
-* ``batched`` / ``served`` streams of mixed instances (orders 3-5).
+* ``batched_instances`` / ``served_stream``: mixed instances (orders 3-4 /
+  3-5, the served ones with Poisson arrival times).
 
 Rules shared by every generator (they make the inferred dims of the written
 ``.tns`` file equal the nominal dims, which the reference derives from the
@@ -43,6 +44,8 @@ __all__ = [
     "write_tns",
     "read_tns_py",
     "batched_instances",
+    "served_stream",
+    "write_quantum",
     "WORKLOADS",
 ]
 
@@ -240,6 +243,45 @@ def batched_instances(count: int = 256, seed: int = 3, max_nnz: int = 1_000_000,
         nnz_y = int(min(nnz_y, cap_y // 4))
         sx = int(rng.integers(0, 2**31))
         params.append((dx, dy, nnz_x, nnz_y, ox, oy, s, sx, nc))
+    return _build_pairs(params, workers)
+
+
+def served_stream(count: int = 256, seed: int = 5, max_nnz: int = 2_000_000, min_nnz: int = 10_000,
+                  nnz_s: float = 1.5, rate: float = 2000.0, max_out_bits: int = 64, workers: int = 0):
+    """Requests of the served workload: operand orders 3-5, 1-2 contract modes,
+    modes log-uniform 64..100k, operand nnz drawn from a power law
+    p(n) ~ n^-nnz_s on [min_nnz, max_nnz] (inverse CDF), contract and free
+    indices Zipf s in [1.0,1.4], U[-1,1) values, Poisson arrivals at ``rate``
+    per second.  Operand keys may exceed 64 bits; instances whose output key
+    would need more than ``max_out_bits`` bits are redrawn.  Returns
+    ``(instances, arrival_seconds)``; instances are ``(X, Y, cx, cy)``."""
+    rng = np.random.default_rng(seed)
+    lo, hi, e = float(min_nnz), float(max_nnz), 1.0 - nnz_s
+
+    def draw_nnz():
+        u = rng.random()
+        return int(round((lo ** e + u * (hi ** e - lo ** e)) ** (1.0 / e)))
+    params = []
+    while len(params) < count:
+        ox = int(rng.integers(3, 6))
+        oy = int(rng.integers(3, 6))
+        nc = int(rng.integers(1, 3))
+        s = float(rng.uniform(1.0, 1.4))
+        logd = lambda: int(round(math.exp(rng.uniform(math.log(64), math.log(100_000)))))  # noqa: E731
+        cdims = [logd() for _ in range(nc)]
+        fx = [logd() for _ in range(ox - nc)]
+        fy = [logd() for _ in range(oy - nc)]
+        if sum(_bits(d) for d in fx) + sum(_bits(d) for d in fy) > max_out_bits:
+            continue
+        dx, dy = fx + cdims, cdims + fy
+        nnz_x = int(min(draw_nnz(), np.prod([float(d) for d in dx]) // 4))
+        nnz_y = int(min(draw_nnz(), np.prod([float(d) for d in dy]) // 4))
+        params.append((dx, dy, nnz_x, nnz_y, ox, oy, s, int(rng.integers(0, 2**31)), nc))
+    arrive = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    return _build_pairs(params, workers), arrive
+
+
+def _build_pairs(params, workers: int):
     if workers == 0:
         workers = min(32, os.cpu_count() or 1)
     total = sum(p[2] + p[3] for p in params)

@@ -246,6 +246,8 @@ typedef struct {
     uint64_t resident_bytes;   /* operands held by the server                               */
     uint64_t peak_reserved_bytes; /* largest working memory admitted at once                */
     uint64_t max_in_flight;    /* most batches running at once                              */
+    uint64_t retries;          /* requests rerun alone after their batch ran out of memory  */
+    uint64_t chunks;           /* output chunks delivered, over all completed requests      */
 } gsparc_server_stats;
 
 gsparc_status gsparc_serve_create(int device, const gsparc_server_opts *opts, gsparc_server **out);

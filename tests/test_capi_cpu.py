@@ -222,3 +222,18 @@ def test_read_quantum_missing_directory():
     with pytest.raises(gb.GsparcError) as e:
         gb.read_quantum("/none/such/dir")
     assert e.value.status == 4
+
+
+def test_served_stream_generator():
+    inst, arrive = synth.served_stream(count=40, seed=2, max_nnz=5_000, min_nnz=500)
+    assert len(inst) == 40 and np.all(np.diff(arrive) > 0)
+    orders = set()
+    for X, Y, cx, cy in inst:
+        orders |= {X.order, Y.order}
+        assert 1 <= len(cx) == len(cy) <= 2
+        assert [X.dims[m] for m in cx] == [Y.dims[m] for m in cy]
+        fx = [d for m, d in enumerate(X.dims) if m not in cx]
+        fy = [d for m, d in enumerate(Y.dims) if m not in cy]
+        assert sum(synth._bits(d) for d in fx + fy) <= 64
+        assert 1 <= X.nnz <= 5_000 and 1 <= Y.nnz <= 5_000
+    assert orders <= {3, 4, 5} and len(orders) >= 2

@@ -197,3 +197,26 @@ def test_small_requests_complete_before_the_batch_ends(ctx, mixed, alone):
         # the batch runs small requests first and is cut after the first
         # large one, so the small requests finish before the last large one
         assert max(r.stats["t_total_ms"] for r in rs) < max(r.stats["t_total_ms"] for r in rb)
+
+
+def test_served_stream_orders_3_to_5_with_wide_keys(ctx):
+    """The served workload's mix (operand orders 3-5, some operand keys over 64
+    bits) through the server: every result equal to the contraction alone."""
+    inst, arrive = synth.served_stream(count=24, seed=8, max_nnz=20_000, min_nnz=2_000)
+    assert {X.order for X, _, _, _ in inst} | {Y.order for _, Y, _, _ in inst} >= {3, 4, 5}
+    with gb.Server(0) as srv:
+        ops = [(srv.upload(X), srv.upload(Y)) for X, Y, _, _ in inst]
+        tickets = []
+        t0 = time.perf_counter()
+        for i, ((dx, dy), (_, _, cx, cy)) in enumerate(zip(ops, inst)):
+            d = t0 + arrive[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(dx, dy, cx, cy))
+        res = [srv.wait(t) for t in tickets]
+    for r, (X, Y, cx, cy) in zip(res, inst):
+        dx, dy = ctx.upload(X), ctx.upload(Y)
+        a = gb.sptc(ctx, dx, dy, cx, cy)
+        dx.free()
+        dy.free()
+        same_result(r, a, X, Y, cx, cy, oracle=X.nnz * Y.nnz < 4e8)
