@@ -87,7 +87,7 @@ EXPORTS = [
     "gsparc_serve_create", "gsparc_serve_destroy", "gsparc_serve_upload", "gsparc_serve_release",
     "gsparc_serve_submit", "gsparc_serve_poll", "gsparc_serve_wait", "gsparc_serve_stats",
     "gsparc_serve_reset_stats", "gsparc_sptc_resident", "gsparc_tensor_download",
-    "gsparc_read_quantum",
+    "gsparc_read_quantum", "gsparc_autotune",
 ]
 
 
@@ -114,6 +114,18 @@ class ServeStats(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("accum", ctypes.c_int), ("max_chunk_nnz", ctypes.c_uint64), ("ms", ctypes.c_double),
+                ("cached", ctypes.c_int), ("ncandidates", ctypes.c_int), ("cand_accum", ctypes.c_int * 8),
+                ("cand_chunk", ctypes.c_uint64 * 8), ("cand_ms", ctypes.c_double * 8)]
+
+    def as_dict(self) -> dict:
+        n = self.ncandidates
+        return {"accum": self.accum, "max_chunk_nnz": self.max_chunk_nnz, "ms": self.ms,
+                "cached": bool(self.cached),
+                "candidates": [(self.cand_accum[i], self.cand_chunk[i], self.cand_ms[i]) for i in range(n)]}
 
 
 class Digest(ctypes.Structure):
@@ -159,6 +171,7 @@ def lib():
     L.gsparc_index_match.argtypes = [P, U64, P, I, U64, P, I, P, P, P, P, P]
     L.gsparc_digest_chunk.argtypes = [P, P, U64, ctypes.POINTER(Digest), P]
     L.gsparc_sptc_batch.argtypes = [P, P, I, U64, ctypes.POINTER(Stats), P]
+    L.gsparc_autotune.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(Tuning), P]
     L.gsparc_sptc_resident.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(P), ctypes.POINTER(Stats), P]
     L.gsparc_serve_create.argtypes = [I, ctypes.POINTER(_ServerOpts), ctypes.POINTER(P)]
     L.gsparc_serve_destroy.argtypes = [P]
@@ -449,6 +462,20 @@ class ResidentResult(DeviceTensor):
         self.order = order.value
         self.dims = [int(d) for d in dims[: self.order]]
         self.nnz = nnz.value
+
+
+def autotune(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: Sequence[int],
+             retune: bool = False, stream: int = 0) -> dict:
+    """Measured choice of accumulator and output chunk size for Z = X x Y
+    (gsparc_autotune): {"accum", "max_chunk_nnz", "ms", "cached", "candidates"}."""
+    if len(cx) != len(cy):
+        raise ValueError("cx and cy must have the same length")
+    c1 = np.asarray(cx, np.int32)
+    c2 = np.asarray(cy, np.int32)
+    t = Tuning()
+    _check(lib().gsparc_autotune(ctx.handle, X.handle, Y.handle, len(c1), _p(c1), _p(c2), int(retune),
+                                 ctypes.byref(t), ctypes.c_void_p(stream)), "autotune")
+    return t.as_dict()
 
 
 def sptc_resident(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: Sequence[int],

@@ -9,6 +9,9 @@
 // reference parses it a second time for this, main.cu:42-48), contracting
 // Z1's last N modes (Y's free modes, the low bits of the reference's Z1 keys
 // that its second contraction matches on) with modes m1..mN of T.
+// -t (extension) measures the accumulator and output chunk size first
+// (gsparc_autotune) and runs the timed iterations with the fastest; it
+// overrides -d.
 // -q reads both operands from the quantum directory format (indices.txt +
 // values.txt, io_manager.tpp:310-484).
 #include <getopt.h>
@@ -35,6 +38,7 @@ struct Opts {
     int multi = 0;
     int na = 0;
     std::vector<int> cz;
+    bool tune = false;
 };
 
 [[noreturn]] void die(const char *what, gsparc_status st) {
@@ -45,7 +49,7 @@ struct Opts {
 void usage(const char *argv0) {
     std::fprintf(stderr,
                  "Usage: %s -X x.tns -Y y.tns -c N -x m1..mN -y m1..mN [-g G] [-n iters] [-d 1|0|-1] [-q]\n"
-                 "          [-m 1 -a K -z t1..tK] [-o z.tns]\n",
+                 "          [-m 1 -a K -z t1..tK] [-t] [-o z.tns]\n",
                  argv0);
 }
 
@@ -195,7 +199,7 @@ int run_multi(const Opts &o, const Tensor &tx, const Tensor &ty) {
 int main(int argc, char **argv) {
     Opts o;
     int c;
-    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhv")) != -1) {
+    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhvt")) != -1) {
         switch (c) {
         case 'X':
             std::fprintf(stderr, "tensor X: %s\n", optarg);
@@ -254,6 +258,9 @@ int main(int argc, char **argv) {
         case 'm':
             o.multi = std::atoi(optarg);
             std::fprintf(stderr, "multi_sptc: %d\n", o.multi);
+            break;
+        case 't':
+            o.tune = true;
             break;
         case 'b':
         case 'v':
@@ -325,8 +332,22 @@ int main(int argc, char **argv) {
                     sink.on_chunk = collect_chunk;
                     sink.user = &parts[g];
                 }
-                s = gsparc_sptc_shard(ctx, X, Y, o.nc, o.cx.data(), o.cy.data(), o.dense, g, o.gpus, &sink,
-                                      &stats[g], nullptr);
+                int accum = o.dense;
+                if (o.tune) {
+                    // measured choice (cached per shape, so only the first iteration pays)
+                    gsparc_tuning tn{};
+                    s = gsparc_autotune(ctx, X, Y, o.nc, o.cx.data(), o.cy.data(), 0, &tn, nullptr);
+                    if (!s) {
+                        accum = tn.accum;
+                        sink.max_chunk_nnz = tn.max_chunk_nnz;
+                        if (it == 0 && g == 0)
+                            std::fprintf(stderr, "autotune: dense_accumulator %d, chunk %llu, %.3f ms\n", tn.accum,
+                                         (unsigned long long)tn.max_chunk_nnz, tn.ms);
+                    }
+                }
+                if (!s)
+                    s = gsparc_sptc_shard(ctx, X, Y, o.nc, o.cx.data(), o.cy.data(), accum, g, o.gpus, &sink,
+                                          &stats[g], nullptr);
             }
             if (X) gsparc_tensor_free(ctx, X);
             if (Y) gsparc_tensor_free(ctx, Y);

@@ -163,6 +163,31 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
                                 int shard, int nshards,
                                 const gsparc_sink *sink, gsparc_stats *stats, void *stream);
 
+/* Measured choice of how to run one contraction.  No counterpart in the
+ * reference, whose accumulator rule is fixed (include/gsparc/sptc.cuh:201-218).
+ * gsparc_autotune runs the contraction (output discarded) with each candidate
+ * -- accumulator ESC or DENSE (rows of up to 1024 products by the on-chip ESC,
+ * or every row by the windowed dense accumulator), and output chunks of the
+ * size the HBM budget allows, a quarter of it and a sixteenth -- times each
+ * with CUDA events on `stream` and returns the fastest.  The choice is
+ * remembered per operand shape (orders, dims, nnz, contract modes) for the
+ * life of the process; a later call for the same shape returns it without
+ * running anything unless `retune` is set.  Pass accum and max_chunk_nnz to
+ * gsparc_sptc / a job's sink. */
+typedef struct {
+    int accum;              /* GSPARC_ACCUM_ESC or GSPARC_ACCUM_DENSE        */
+    uint64_t max_chunk_nnz; /* 0 = from the HBM budget                       */
+    double ms;              /* measured time of the choice                   */
+    int cached;             /* 1: taken from the cache, nothing was run      */
+    int ncandidates;
+    int cand_accum[8];
+    uint64_t cand_chunk[8];
+    double cand_ms[8];
+} gsparc_tuning;
+gsparc_status gsparc_autotune(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y,
+                              int ncmodes, const int *cx, const int *cy, int retune,
+                              gsparc_tuning *out, void *stream);
+
 /* Z = X x_{cx,cy} Y kept on the device as a resident COO tensor: its modes
  * are X's free modes (ascending) followed by Y's free modes (ascending), and
  * it can be an operand of any later contraction (free it with

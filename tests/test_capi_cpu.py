@@ -35,7 +35,8 @@ def test_ctypes_structs_match_the_header(tmp_path):
     from gsparc_b200 import api
     structs = {"gsparc_coo": api._Coo, "gsparc_sink": api._Sink, "gsparc_stats": api.Stats,
                "gsparc_job": api._Job, "gsparc_digest": api.Digest,
-               "gsparc_server_opts": api._ServerOpts, "gsparc_server_stats": api.ServeStats}
+               "gsparc_server_opts": api._ServerOpts, "gsparc_server_stats": api.ServeStats,
+               "gsparc_tuning": api.Tuning}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "gsparc_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
