@@ -87,7 +87,9 @@ EXPORTS = [
     "gsparc_serve_create", "gsparc_serve_destroy", "gsparc_serve_upload", "gsparc_serve_release",
     "gsparc_serve_submit", "gsparc_serve_poll", "gsparc_serve_wait", "gsparc_serve_stats",
     "gsparc_serve_reset_stats", "gsparc_sptc_resident", "gsparc_tensor_download",
-    "gsparc_read_quantum", "gsparc_autotune",
+    "gsparc_read_quantum", "gsparc_autotune", "gsparc_plan_create", "gsparc_plan_chunks", "gsparc_plan_chunk",
+    "gsparc_plan_job_output", "gsparc_plan_refresh", "gsparc_plan_execute", "gsparc_plan_check",
+    "gsparc_plan_destroy", "gsparc_tensor_set_values",
 ]
 
 
@@ -171,6 +173,15 @@ def lib():
     L.gsparc_index_match.argtypes = [P, U64, P, I, U64, P, I, P, P, P, P, P]
     L.gsparc_digest_chunk.argtypes = [P, P, U64, ctypes.POINTER(Digest), P]
     L.gsparc_sptc_batch.argtypes = [P, P, I, U64, ctypes.POINTER(Stats), P]
+    L.gsparc_plan_create.argtypes = [P, P, I, U64, ctypes.POINTER(P), ctypes.POINTER(U64), P]
+    L.gsparc_plan_chunks.argtypes = [P, ctypes.POINTER(U64)]
+    L.gsparc_plan_chunk.argtypes = [P, U64, ctypes.POINTER(U64), ctypes.POINTER(U64)]
+    L.gsparc_plan_job_output.argtypes = [P, I, ctypes.POINTER(U64), ctypes.POINTER(U64)]
+    L.gsparc_plan_refresh.argtypes = [P, P]
+    L.gsparc_plan_execute.argtypes = [P, U64, P, P, U64, P]
+    L.gsparc_plan_check.argtypes = [P, P]
+    L.gsparc_plan_destroy.argtypes = [P]
+    L.gsparc_tensor_set_values.argtypes = [P, P, P, I, P]
     L.gsparc_autotune.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(Tuning), P]
     L.gsparc_sptc_resident.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(P), ctypes.POINTER(Stats), P]
     L.gsparc_serve_create.argtypes = [I, ctypes.POINTER(_ServerOpts), ctypes.POINTER(P)]
@@ -338,6 +349,14 @@ class DeviceTensor:
     def handle(self):
         return self._h
 
+    def set_values(self, val: np.ndarray, stream: int = 0) -> None:
+        """Overwrite the values (same order as the uploaded COO), coordinates unchanged."""
+        v = np.ascontiguousarray(val, np.float32)
+        if v.shape[0] != self.nnz:
+            raise ValueError("need one value per nonzero")
+        _check(lib().gsparc_tensor_set_values(self.ctx.handle, self._h, _p(v), 0, ctypes.c_void_p(stream)),
+               "tensor_set_values")
+
     def download(self) -> CooTensor:
         """Copy the tensor back to host memory."""
         idx = np.zeros((self.order, self.nnz), np.uint64)
@@ -462,6 +481,73 @@ class ResidentResult(DeviceTensor):
         self.order = order.value
         self.dims = [int(d) for d in dims[: self.order]]
         self.nnz = nnz.value
+
+
+class Plan:
+    """Coordinate-only work of one or more contractions done once
+    (gsparc_plan_*); ``execute(k, keys, vals)`` replays the numeric pass of
+    output chunk k into device arrays (torch tensors or raw pointers) with
+    launches only, so it can be captured in a CUDA graph.  ``refresh()`` picks
+    up operand values changed with ``DeviceTensor.set_values``."""
+
+    def __init__(self, ctx: Context, jobs, max_chunk_nnz: int = 0, stream: int = 0):
+        self.ctx = ctx
+        n = len(jobs)
+        arr = (_Job * n)()
+        self._keep = []
+        for j, job in enumerate(jobs):
+            X, Y, cx, cy = job[:4]
+            c1 = np.asarray(cx, np.int32)
+            c2 = np.asarray(cy, np.int32)
+            self._keep += [c1, c2, X, Y]
+            arr[j].x, arr[j].y = X.handle, Y.handle
+            arr[j].ncmodes = len(c1)
+            arr[j].cx, arr[j].cy = c1.ctypes.data, c2.ctypes.data
+            arr[j].accum = int(job[4]) if len(job) > 4 else ACCUM_AUTO
+        self._h = ctypes.c_void_p()
+        tot = ctypes.c_uint64()
+        _check(lib().gsparc_plan_create(ctx.handle, ctypes.cast(arr, ctypes.c_void_p), n, max_chunk_nnz,
+                                        ctypes.byref(self._h), ctypes.byref(tot), ctypes.c_void_p(stream)),
+               "plan_create")
+        self.total = tot.value
+        nc = ctypes.c_uint64()
+        _check(lib().gsparc_plan_chunks(self._h, ctypes.byref(nc)), "plan_chunks")
+        self.nchunks = nc.value
+        self.njobs = n
+
+    def chunk(self, k: int):
+        f, m = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().gsparc_plan_chunk(self._h, k, ctypes.byref(f), ctypes.byref(m)), "plan_chunk")
+        return f.value, m.value
+
+    def job_output(self, j: int):
+        f, m = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().gsparc_plan_job_output(self._h, j, ctypes.byref(f), ctypes.byref(m)), "plan_job_output")
+        return f.value, m.value
+
+    def refresh(self, stream: int = 0):
+        _check(lib().gsparc_plan_refresh(self._h, ctypes.c_void_p(stream)), "plan_refresh")
+
+    def execute(self, k: int, keys, vals, stream: int = 0):
+        kp = keys.data_ptr() if hasattr(keys, "data_ptr") else int(keys)
+        vp = vals.data_ptr() if hasattr(vals, "data_ptr") else int(vals)
+        cap = min(keys.numel(), vals.numel()) if hasattr(keys, "numel") else self.chunk(k)[1]
+        _check(lib().gsparc_plan_execute(self._h, k, ctypes.c_void_p(kp), ctypes.c_void_p(vp), cap,
+                                         ctypes.c_void_p(stream)), "plan_execute")
+
+    def check(self, stream: int = 0):
+        _check(lib().gsparc_plan_check(self._h, ctypes.c_void_p(stream)), "plan_check")
+
+    def close(self):
+        if self._h:
+            _check(lib().gsparc_plan_destroy(self._h), "plan_destroy")
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def autotune(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: Sequence[int],

@@ -89,7 +89,7 @@ struct JobOut {
 // damage its own job's keys.
 __global__ void k_blin(const BLin *__restrict__ tab, const uint64_t *__restrict__ offs, int g,
                        uint64_t total, int kb, uint64_t *__restrict__ keys, float *__restrict__ vals,
-                       unsigned int *__restrict__ jerr) {
+                       unsigned int *__restrict__ jerr, int perm) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t km = low_mask(kb);
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += stride) {
@@ -116,7 +116,27 @@ __global__ void k_blin(const BLin *__restrict__ tab, const uint64_t *__restrict_
         if (bad) atomicOr(&jerr[lo], 1u);
         const uint64_t key = t.p.role == 0 ? (shl(f, t.p.ncbits) | c) : (shl(c, t.p.nfbits) | f);
         keys[k] = shl((uint64_t)lo, kb) | (key & km);
-        vals[k] = t.val[l];
+        // with perm the sort carries each entry's input position instead of its value
+        vals[k] = perm ? __uint_as_float((unsigned int)k) : t.val[l];
+    }
+}
+
+// The current values of sorted entries whose input positions the sort carried
+// (k_blin with perm): vals[i] = the value at input position perm[i].
+__global__ void k_bvals(const BLin *__restrict__ tab, const uint64_t *__restrict__ offs, int g, uint64_t total,
+                        const float *__restrict__ perm, float *__restrict__ vals) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const uint64_t k = __float_as_uint(perm[i]);
+        int lo = 0, hi = g;  // largest j with offs[j] <= k
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (offs[mid] <= k)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        vals[i] = tab[lo].val[k - offs[lo]];
     }
 }
 
@@ -594,6 +614,32 @@ struct Times {
     double lin = 0, sort = 0, match = 0, plan = 0, contract = 0, out = 0, total = 0, numeric = 0;
 };
 
+// Everything the numeric pass of one group needs, kept on the device by a plan
+// (gsparc_plan_*): the sorted operands' positions and current values, the run
+// table, the match, the rows, the unit lists and the output offsets.
+struct GroupPlan {
+    int g = 0;
+    uint64_t nx = 0, ny = 0, ntot = 0, nu = 0, nh = 0, nsr = 0;
+    int gl = 1, gh = 1, gs_grid = 1;
+    AccArgs aa{};
+    std::vector<uint64_t> job_first;  // g + 1 group-local output offsets
+    std::vector<Job *> jobs;
+    DBuf<BLin> d_lx, d_ly;
+    DBuf<uint64_t> d_xoffs, d_yoffs;
+    DBuf<float> xperm, yperm, xvals, yvals;
+    DBuf<BatchJob> d_acc;
+    DBuf<uint32_t> rank, pos, cnt, row_start, units, H, H2, SR, row_xi, cursor, pend;
+    DBuf<uint64_t> cols, xprefix, row_xf, sprefix, row_off;
+    DBuf<uint16_t> row_job;
+    DBuf<uint32_t> Hc;         // heavy rows grouped by chunk (several chunks only)
+    DBuf<unsigned int> flags;  // error bits, work counter, windows swept, spare
+    struct Chunk {
+        uint64_t lu0, lu1, h0, h1, s0, s1, first, n;
+    };
+    std::vector<Chunk> chunks;
+    const uint32_t *heavy_list() const { return Hc.get() ? Hc.get() : (H2.get() ? H2.get() : H.get()); }
+};
+
 // Delivers [dk, dk + n) of a job's output (first = offset inside the job).
 void deliver_slice(gsparc_sink &sink, const uint64_t *dk, const float *dv, uint64_t n, uint64_t first,
                    uint64_t job_nnz, cudaStream_t s2, gsparc_stats &st, uint64_t &bytes_d2h) {
@@ -630,7 +676,7 @@ void deliver_slice(gsparc_sink &sink, const uint64_t *dk, const float *dv, uint6
 }
 
 void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, int shard, int nshards,
-               Times &tm, gsparc_stats &bst, cudaStream_t s, const JobDoneFn *done_fn) {
+               Times &tm, gsparc_stats &bst, cudaStream_t s, const JobDoneFn *done_fn, GroupPlan *keep = nullptr) {
     Arena &A = ctx->arena;
     const int g = (int)G.size();
     const int jb = ceil_log2((uint64_t)g);
@@ -687,12 +733,12 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     DBuf<uint64_t> xk0(A, nx, s), xk1(A, nx, s), yk0(A, ny, s), yk1(A, ny, s);
     DBuf<float> xv0(A, nx, s), xv1(A, nx, s), yv0(A, ny, s), yv1(A, ny, s);
     if (nx) {
-        k_blin<<<grid_for(nx), kThreads, 0, s>>>(d_lx, d_xoffs, g, nx, kbx, xk0, xv0, d_jerr);
+        k_blin<<<grid_for(nx), kThreads, 0, s>>>(d_lx, d_xoffs, g, nx, kbx, xk0, xv0, d_jerr, keep != nullptr);
         count_launch();
         GS_CUDA(cudaGetLastError());
     }
     if (ny) {
-        k_blin<<<grid_for(ny), kThreads, 0, s>>>(d_ly, d_yoffs, g, ny, kby, yk0, yv0, d_jerr);
+        k_blin<<<grid_for(ny), kThreads, 0, s>>>(d_ly, d_yoffs, g, ny, kby, yk0, yv0, d_jerr, keep != nullptr);
         count_launch();
         GS_CUDA(cudaGetLastError());
     }
@@ -708,6 +754,19 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     const float *yvals = wy ? yv1.get() : yv0.get();
     if (wx) { xk0.release(); xv0.release(); } else { xk1.release(); xv1.release(); }
     if (wy) { yk0.release(); yv0.release(); } else { yk1.release(); yv1.release(); }
+    if (keep) {
+        // the sorted "values" are input positions: keep them, fetch the values
+        keep->xperm = wx ? std::move(xv1) : std::move(xv0);
+        keep->yperm = wy ? std::move(yv1) : std::move(yv0);
+        keep->xvals.reset(A, std::max<uint64_t>(nx, 1), s);
+        keep->yvals.reset(A, std::max<uint64_t>(ny, 1), s);
+        if (nx) k_bvals<<<grid_for(nx), kThreads, 0, s>>>(d_lx, d_xoffs, g, nx, keep->xperm, keep->xvals);
+        if (ny) k_bvals<<<grid_for(ny), kThreads, 0, s>>>(d_ly, d_yoffs, g, ny, keep->yperm, keep->yvals);
+        count_launch((nx ? 1 : 0) + (ny ? 1 : 0));
+        GS_CUDA(cudaGetLastError());
+        xvals = keep->xvals.get();
+        yvals = keep->yvals.get();
+    }
     mark(2);
 
     // ---- Y column tables, ranks and run table ----
@@ -1033,6 +1092,61 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     }
     bst.chunks += chunks.size();
 
+    if (keep) {
+        // a plan keeps what the numeric pass needs and stops here
+        keep->g = g;
+        keep->nx = nx;
+        keep->ny = ny;
+        keep->ntot = ntot;
+        keep->nu = nu;
+        keep->nh = nh;
+        keep->nsr = nsr;
+        keep->gl = gl;
+        keep->gh = gh;
+        keep->gs_grid = gs_grid;
+        keep->job_first.resize(g + 1);
+        for (int j = 0; j <= g; ++j) keep->job_first[j] = jo[j].out_off;
+        keep->jobs = G;
+        keep->d_lx = std::move(d_lx);
+        keep->d_ly = std::move(d_ly);
+        keep->d_xoffs = std::move(d_xoffs);
+        keep->d_yoffs = std::move(d_yoffs);
+        keep->d_acc = std::move(d_acc);
+        keep->rank = std::move(rank);
+        keep->pos = std::move(pos);
+        keep->cnt = std::move(cnt);
+        keep->row_start = std::move(row_start);
+        keep->units = std::move(units);
+        keep->H = std::move(H);
+        keep->H2 = std::move(H2);
+        keep->SR = std::move(SR);
+        keep->row_xi = std::move(row_xi);
+        keep->cursor = std::move(cursor);
+        keep->pend = std::move(pend);
+        keep->cols = std::move(cols);
+        keep->xprefix = std::move(xprefix);
+        keep->row_xf = std::move(row_xf);
+        keep->sprefix = std::move(sprefix);
+        keep->row_off = std::move(row_off);
+        keep->row_job = std::move(row_job);
+        keep->Hc = std::move(Hc);
+        keep->chunks.clear();
+        for (auto &c : chunks) keep->chunks.push_back({c.lu0, c.lu1, c.h0, c.h1, c.s0, c.s1, c.first, c.n});
+        keep->flags.reset(A, 4, s);
+        GS_CUDA(cudaMemsetAsync(keep->flags.get(), 0, 16, s));
+        keep->aa = aa;  // the moved buffers keep their device addresses
+        keep->aa.err = keep->flags.get();
+        keep->aa.work_counter = keep->flags.get() + 1;
+        keep->aa.row_nnz = nullptr;  // the symbolic counts are not kept
+        GS_CUDA(cudaStreamSynchronize(s));
+        tm.lin += ms(0, 1);
+        tm.sort += ms(1, 2);
+        tm.match += ms(2, 3);
+        tm.plan += ms(3, 4);
+        tm.total += ms(0, 4);
+        return;
+    }
+
     // ---- numeric pass, chunk by chunk, double-buffered against delivery ----
     const int nbuf = chunks.size() > 1 ? 2 : 1;
     uint64_t bufn = 0;
@@ -1149,18 +1263,10 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
 
 }  // namespace
 
-void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st_out,
-                cudaStream_t s, int shard, int nshards, const JobDoneFn *done_fn) {
-    GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
-    GS_REQUIRE(njobs >= 0 && (njobs == 0 || jobs), GSPARC_EINVAL, "bad job array");
-    GS_REQUIRE(nshards >= 1 && shard >= 0 && shard < nshards, GSPARC_EINVAL, "bad shard");
-    GS_REQUIRE(nshards == 1 || njobs == 1, GSPARC_EINVAL, "row shards apply to a single contraction");
-    gsparc_stats bst;
-    std::memset(&bst, 0, sizeof(bst));
-    const uint64_t launches0 = launch_count();
-
-    // validate every job on its own; a bad job fails alone
-    std::vector<Job> js;
+// Checks every job on its own (a bad job fails alone: its status says why)
+// and prepares the ones that pass: layouts, relabeling of keys over 64 bits.
+void validate_jobs(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, cudaStream_t s, std::vector<Job> &js,
+                   gsparc_stats &bst) {
     js.reserve(njobs);
     for (int i = 0; i < njobs; ++i) {
         gsparc_job &J = jobs[i];
@@ -1218,7 +1324,11 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
         }
     }
 
-    // groups: widest keys first; a group of n jobs needs ceil(log2 n) id bits
+}
+
+// Groups of jobs whose keys, with the job id above them, fit 64 bits: widest
+// keys first; a group of n jobs needs ceil(log2 n) id bits.
+std::vector<std::vector<Job *>> make_groups(std::vector<Job> &js) {
     std::vector<Job *> order;
     for (auto &q : js) order.push_back(&q);
     std::stable_sort(order.begin(), order.end(), [](const Job *a, const Job *b) { return a->width > b->width; });
@@ -1243,6 +1353,23 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
             groups.push_back(std::move(G));
         }
     }
+
+    return groups;
+}
+
+void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st_out,
+                cudaStream_t s, int shard, int nshards, const JobDoneFn *done_fn) {
+    GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+    GS_REQUIRE(njobs >= 0 && (njobs == 0 || jobs), GSPARC_EINVAL, "bad job array");
+    GS_REQUIRE(nshards >= 1 && shard >= 0 && shard < nshards, GSPARC_EINVAL, "bad shard");
+    GS_REQUIRE(nshards == 1 || njobs == 1, GSPARC_EINVAL, "row shards apply to a single contraction");
+    gsparc_stats bst;
+    std::memset(&bst, 0, sizeof(bst));
+    const uint64_t launches0 = launch_count();
+
+    std::vector<Job> js;
+    validate_jobs(ctx, jobs, njobs, s, js, bst);
+    std::vector<std::vector<Job *>> groups = make_groups(js);
 
     // completion reports: at most one per job, early ones from run_group
     std::vector<char> reported(njobs, 0);
@@ -1300,6 +1427,164 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
             fail(jobs[i].status, std::string("job ") + std::to_string(i) + " failed (" +
                                      gsparc_status_string(jobs[i].status) + "); last message: " + last_error());
         }
+}
+
+}  // namespace gs
+
+// ---- plans: the coordinate-only work done once, the numeric pass replayed ----
+
+struct gsparc_plan {
+    gsparc_ctx *ctx = nullptr;
+    std::vector<gsparc_job> jobs;  // copies of the caller's jobs (modes copied too)
+    std::vector<std::vector<int>> modes;
+    std::vector<gs::Job> js;
+    std::vector<std::unique_ptr<gs::GroupPlan>> groups;
+    std::vector<uint64_t> group_off;               // first output of each group
+    std::vector<std::pair<int, int>> chunk_of;     // plan chunk -> (group, group chunk)
+    std::vector<uint64_t> job_first, job_nnz;      // per caller job
+    uint64_t total = 0;
+};
+
+namespace gs {
+
+void plan_create(gsparc_ctx *ctx, const gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_plan **out,
+                 uint64_t *total, cudaStream_t s) {
+    GS_REQUIRE(ctx && out && njobs >= 1 && jobs, GSPARC_EINVAL, "bad argument");
+    *out = nullptr;
+    auto P = std::make_unique<gsparc_plan>();
+    P->ctx = ctx;
+    P->jobs.assign(jobs, jobs + njobs);
+    P->modes.resize(njobs);
+    for (int i = 0; i < njobs; ++i) {
+        gsparc_job &J = P->jobs[i];
+        GS_REQUIRE(J.ncmodes >= 1 && J.ncmodes <= kMaxOrder && J.cx && J.cy, GSPARC_EINVAL, "bad contract modes");
+        auto &m = P->modes[i];
+        m.assign(J.cx, J.cx + J.ncmodes);
+        m.insert(m.end(), J.cy, J.cy + J.ncmodes);
+        J.cx = m.data();
+        J.cy = m.data() + J.ncmodes;
+        J.sink = gsparc_sink{};
+        J.sink.kind = GSPARC_SINK_DISCARD;
+    }
+    gsparc_stats bst;
+    std::memset(&bst, 0, sizeof(bst));
+    validate_jobs(ctx, P->jobs.data(), njobs, s, P->js, bst);
+    for (int i = 0; i < njobs; ++i)
+        if (P->jobs[i].status != GSPARC_OK)
+            fail(P->jobs[i].status, "job " + std::to_string(i) + ": " + last_error());
+    std::vector<std::vector<Job *>> groups = make_groups(P->js);
+    Times tm;
+    P->job_first.assign(njobs, 0);
+    P->job_nnz.assign(njobs, 0);
+    for (auto &G : groups) {
+        auto gp = std::make_unique<GroupPlan>();
+        run_group(ctx, G, max_chunk_nnz, 0, 1, tm, bst, s, nullptr, gp.get());
+        for (Job *q : G)
+            if (q->job->status != GSPARC_OK) fail(q->job->status, last_error());
+        P->group_off.push_back(P->total);
+        for (size_t c = 0; c < gp->chunks.size(); ++c) P->chunk_of.push_back({(int)P->groups.size(), (int)c});
+        for (int j = 0; j < gp->g; ++j) {
+            const int i = (int)(gp->jobs[j]->job - P->jobs.data());
+            P->job_first[i] = P->total + gp->job_first[j];
+            P->job_nnz[i] = gp->job_first[j + 1] - gp->job_first[j];
+        }
+        P->total += gp->ntot;
+        P->groups.push_back(std::move(gp));
+    }
+    if (total) *total = P->total;
+    *out = P.release();
+}
+
+// One chunk of a plan's output into keys/vals (first = the chunk's first
+// output).  Launches only: memsets, value gathers, the numeric kernels and
+// (for jobs with keys over 64 bits) the output key map.
+void plan_execute(gsparc_plan *P, uint64_t chunk, uint64_t *keys, float *vals, uint64_t capacity,
+                  cudaStream_t s) {
+    GS_REQUIRE(P && chunk < P->chunk_of.size(), GSPARC_EINVAL, "no such chunk");
+    const int gi = P->chunk_of[chunk].first, ci = P->chunk_of[chunk].second;
+    GroupPlan &gp = *P->groups[gi];
+    const GroupPlan::Chunk &c = gp.chunks[ci];
+    GS_REQUIRE(c.n <= capacity && (c.n == 0 || (keys && vals)), GSPARC_EINVAL,
+               "output arrays smaller than the chunk (gsparc_plan_chunk gives its size)");
+    AccArgs b = gp.aa;
+    b.chunk_base = c.first;
+    b.out_keys = keys;
+    b.out_vals = vals;
+    b.out_cap = c.n;
+    b.units = gp.units.get() + 2 * c.lu0;
+    b.nunits = (uint32_t)(c.lu1 - c.lu0);
+    GS_CUDA(cudaMemsetAsync(gp.flags.get() + 1, 0, 4, s));
+    launch_light(b, true, (int)std::min<uint64_t>(gp.gl, std::max<uint64_t>(1, b.nunits)), s);
+    b.units = gp.heavy_list() + c.h0;
+    b.nunits = (uint32_t)(c.h1 - c.h0);
+    GS_CUDA(cudaMemsetAsync(gp.flags.get() + 1, 0, 4, s));
+    launch_heavy(b, true, (int)std::min<uint64_t>(gp.gh, std::max<uint64_t>(1, b.nunits)), s);
+    b.units = gp.SR.get() + c.s0;
+    b.nunits = (uint32_t)(c.s1 - c.s0);
+    b.sprefix = gp.sprefix.get() + c.s0;
+    launch_stream(b, gp.gs_grid, s);
+    for (int j = 0; j < gp.g; ++j) {
+        if (!gp.jobs[j]->wide) continue;
+        const uint64_t a0 = std::max(c.first, gp.job_first[j]), a1 = std::min(c.first + c.n, gp.job_first[j + 1]);
+        if (a1 > a0) wide_remap_keys(*gp.jobs[j]->wide, keys + (a0 - c.first), a1 - a0, s);
+    }
+}
+
+// Fetches the operands' current values into the plan's sorted value arrays.
+void plan_refresh(gsparc_plan *P, cudaStream_t s) {
+    GS_REQUIRE(P, GSPARC_EINVAL, "null plan");
+    for (auto &g : P->groups) {
+        GroupPlan &gp = *g;
+        if (gp.nx) {
+            k_bvals<<<grid_for(gp.nx), kThreads, 0, s>>>(gp.d_lx, gp.d_xoffs, gp.g, gp.nx, gp.xperm, gp.xvals);
+            count_launch();
+        }
+        if (gp.ny) {
+            k_bvals<<<grid_for(gp.ny), kThreads, 0, s>>>(gp.d_ly, gp.d_yoffs, gp.g, gp.ny, gp.yperm, gp.yvals);
+            count_launch();
+        }
+        GS_CUDA(cudaGetLastError());
+    }
+}
+
+// Waits for `s`, reads and clears the device-side error words of every group.
+void plan_check(gsparc_plan *P, cudaStream_t s) {
+    GS_REQUIRE(P, GSPARC_EINVAL, "null plan");
+    for (auto &gp : P->groups) {
+        unsigned int f = 0;
+        d2h(&f, gp->flags.get(), 1, s);
+        GS_CUDA(cudaMemsetAsync(gp->flags.get(), 0, 4, s));
+        GS_CUDA(cudaStreamSynchronize(s));
+        GS_REQUIRE(!(f & 2u), GSPARC_EINTERNAL, "light unit over capacity");
+        GS_REQUIRE(!(f & 4u), GSPARC_EINTERNAL, "numeric pass wrote past its chunk");
+    }
+}
+
+void plan_destroy(gsparc_plan *P) {
+    if (!P) return;
+    const int dev = P->ctx->device;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+    cudaDeviceSynchronize();  // the buffers may still be read by executions in flight
+    delete P;
+    if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+}
+
+uint64_t plan_nchunks(const gsparc_plan *P) { return P->chunk_of.size(); }
+
+void plan_chunk(const gsparc_plan *P, uint64_t k, uint64_t *first, uint64_t *nnz) {
+    GS_REQUIRE(k < P->chunk_of.size(), GSPARC_EINVAL, "no such chunk");
+    const GroupPlan &gp = *P->groups[P->chunk_of[k].first];
+    const GroupPlan::Chunk &c = gp.chunks[P->chunk_of[k].second];
+    if (first) *first = P->group_off[P->chunk_of[k].first] + c.first;
+    if (nnz) *nnz = c.n;
+}
+
+void plan_job_output(const gsparc_plan *P, int job, uint64_t *first, uint64_t *nnz) {
+    GS_REQUIRE(job >= 0 && job < (int)P->job_first.size(), GSPARC_EINVAL, "no such job");
+    if (first) *first = P->job_first[job];
+    if (nnz) *nnz = P->job_nnz[job];
 }
 
 }  // namespace gs

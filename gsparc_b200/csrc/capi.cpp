@@ -256,6 +256,66 @@ gsparc_status gsparc_sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, ui
     });
 }
 
+gsparc_status gsparc_plan_create(gsparc_ctx *ctx, const gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz,
+                                 gsparc_plan **out, uint64_t *total_nnz, void *stream) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        DeviceScope ds(ctx->device);
+        gs::plan_create(ctx, jobs, njobs, max_chunk_nnz, out, total_nnz, (cudaStream_t)stream);
+    });
+}
+
+gsparc_status gsparc_plan_chunks(const gsparc_plan *plan, uint64_t *nchunks) {
+    return guard([&] {
+        GS_REQUIRE(plan && nchunks, GSPARC_EINVAL, "null argument");
+        *nchunks = gs::plan_nchunks(plan);
+    });
+}
+
+gsparc_status gsparc_plan_chunk(const gsparc_plan *plan, uint64_t k, uint64_t *first, uint64_t *nnz) {
+    return guard([&] {
+        GS_REQUIRE(plan, GSPARC_EINVAL, "null plan");
+        gs::plan_chunk(plan, k, first, nnz);
+    });
+}
+
+gsparc_status gsparc_plan_job_output(const gsparc_plan *plan, int job, uint64_t *first, uint64_t *nnz) {
+    return guard([&] {
+        GS_REQUIRE(plan, GSPARC_EINVAL, "null plan");
+        gs::plan_job_output(plan, job, first, nnz);
+    });
+}
+
+gsparc_status gsparc_plan_refresh(gsparc_plan *plan, void *stream) {
+    return guard([&] { gs::plan_refresh(plan, (cudaStream_t)stream); });
+}
+
+gsparc_status gsparc_plan_execute(gsparc_plan *plan, uint64_t k, uint64_t *d_keys, float *d_vals,
+                                  uint64_t capacity, void *stream) {
+    return guard([&] { gs::plan_execute(plan, k, d_keys, d_vals, capacity, (cudaStream_t)stream); });
+}
+
+gsparc_status gsparc_plan_check(gsparc_plan *plan, void *stream) {
+    return guard([&] { gs::plan_check(plan, (cudaStream_t)stream); });
+}
+
+gsparc_status gsparc_plan_destroy(gsparc_plan *plan) {
+    return guard([&] { gs::plan_destroy(plan); });
+}
+
+gsparc_status gsparc_tensor_set_values(gsparc_ctx *ctx, gsparc_tensor *t, const float *val, int on_device,
+                                       void *stream) {
+    return guard([&] {
+        GS_REQUIRE(ctx && t && (t->nnz == 0 || val), GSPARC_EINVAL, "null argument");
+        DeviceScope ds(ctx->device);
+        cudaStream_t s = (cudaStream_t)stream;
+        if (t->nnz)
+            GS_CUDA(cudaMemcpyAsync(t->d_val, val, 4 * t->nnz,
+                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+        GS_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 gsparc_status gsparc_read_tns(const char *path, int nthreads, int *order, uint64_t *dims, uint64_t *nnz,
                               uint64_t **idx, float **val) {
     return guard([&] {

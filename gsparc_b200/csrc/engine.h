@@ -25,6 +25,17 @@ void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk
 void sptc_resident(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int nc, const int *cx,
                    const int *cy, int accum, gsparc_tensor **out, gsparc_stats *stats, cudaStream_t s);
 
+// Plans (batch.cu): coordinate-only work done once, the numeric pass replayed.
+void plan_create(gsparc_ctx *ctx, const gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_plan **out,
+                 uint64_t *total, cudaStream_t s);
+void plan_refresh(gsparc_plan *P, cudaStream_t s);
+void plan_execute(gsparc_plan *P, uint64_t chunk, uint64_t *keys, float *vals, uint64_t capacity, cudaStream_t s);
+void plan_check(gsparc_plan *P, cudaStream_t s);
+void plan_destroy(gsparc_plan *P);
+uint64_t plan_nchunks(const gsparc_plan *P);
+void plan_chunk(const gsparc_plan *P, uint64_t k, uint64_t *first, uint64_t *nnz);
+void plan_job_output(const gsparc_plan *P, int job, uint64_t *first, uint64_t *nnz);
+
 void plan_shards(const uint64_t *row_prod, uint64_t nrows, int nshards, uint64_t *bounds);
 
 // .tns text I/O (tns_io.cpp)

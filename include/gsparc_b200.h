@@ -229,6 +229,42 @@ typedef struct {
 gsparc_status gsparc_sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz,
                                 gsparc_stats *stats, void *stream);
 
+/* ---- plans: coordinates once, values many times -------------------------- */
+/* No counterpart in the reference, which redoes every step per call.  A plan
+ * does, once, everything of a set of contractions that depends only on the
+ * operands' coordinates -- linearise, sort, run table, match, row planning,
+ * the symbolic pass and the output chunks (at most max_chunk_nnz outputs each,
+ * 0 = from the HBM budget) -- and keeps it on the device.  Executing a chunk
+ * runs only the numeric pass into caller-provided device arrays: memsets and
+ * kernel launches on `stream`, no allocation, no host synchronisation, so a
+ * caller may capture its executions in a CUDA graph and replay them.
+ * gsparc_plan_refresh fetches the operands' current values (after
+ * gsparc_tensor_set_values); the coordinates must stay those the plan was
+ * made from.  The plan holds the context's memory until destroyed; destroy it
+ * before the context and the tensors.  The jobs' sinks are ignored; job i's
+ * output is the range gsparc_plan_job_output gives of the plan's output,
+ * whose chunks are consecutive. */
+typedef struct gsparc_plan gsparc_plan;
+gsparc_status gsparc_plan_create(gsparc_ctx *ctx, const gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz,
+                                 gsparc_plan **out, uint64_t *total_nnz, void *stream);
+/* Number of output chunks, and chunk k's first output and size. */
+gsparc_status gsparc_plan_chunks(const gsparc_plan *plan, uint64_t *nchunks);
+gsparc_status gsparc_plan_chunk(const gsparc_plan *plan, uint64_t k, uint64_t *first, uint64_t *nnz);
+/* Job i's output: `first` (in the plan's output) and nnz. */
+gsparc_status gsparc_plan_job_output(const gsparc_plan *plan, int job, uint64_t *first, uint64_t *nnz);
+gsparc_status gsparc_plan_refresh(gsparc_plan *plan, void *stream);
+/* Chunk k into d_keys/d_vals (device arrays of at least the chunk's size). */
+gsparc_status gsparc_plan_execute(gsparc_plan *plan, uint64_t k, uint64_t *d_keys, float *d_vals,
+                                  uint64_t capacity, void *stream);
+/* Waits for `stream`; reports (and clears) a device-side check that failed in
+ * the executions since the last check. */
+gsparc_status gsparc_plan_check(gsparc_plan *plan, void *stream);
+gsparc_status gsparc_plan_destroy(gsparc_plan *plan);
+/* Overwrite a resident tensor's values (nnz of them, in the order of the COO
+ * it was uploaded from; host or device memory), coordinates unchanged. */
+gsparc_status gsparc_tensor_set_values(gsparc_ctx *ctx, gsparc_tensor *t, const float *val, int on_device,
+                                       void *stream);
+
 /* ---- serving: a request loop over resident operands ----------------------- */
 /* No counterpart in the reference, which runs one contraction per process
  * (main.cu:22-437).  A server owns one device, an HBM budget shared by its
