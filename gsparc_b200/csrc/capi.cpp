@@ -84,6 +84,7 @@ gsparc_status gsparc_ctx_create(int device, uint64_t budget, gsparc_ctx **out) {
             for (auto &e : ctx->ev) GS_CUDA(cudaEventCreate(&e));
             GS_CUDA(cudaMalloc(&ctx->d_flag, 64));
             GS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+            GS_CUDA(cudaStreamCreateWithFlags(&ctx->alt_stream, cudaStreamNonBlocking));
             GS_CUDA(cudaMemset(ctx->d_flag, 0, 64));
         } catch (...) {
             delete ctx;
@@ -102,6 +103,7 @@ gsparc_status gsparc_ctx_destroy(gsparc_ctx *ctx) {
             if (e) cudaEventDestroy(e);
         if (ctx->d_flag) cudaFree(ctx->d_flag);
         if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+        if (ctx->alt_stream) cudaStreamDestroy(ctx->alt_stream);
         delete ctx;
     });
 }

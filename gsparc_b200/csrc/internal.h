@@ -136,6 +136,7 @@ struct gsparc_ctx {
     cudaEvent_t ev[16] = {};
     unsigned int *d_flag = nullptr;  // device error / work counters
     cudaStream_t copy_stream = nullptr;  // output chunk copies (non-blocking)
+    cudaStream_t alt_stream = nullptr;   // every other output chunk's kernels (non-blocking)
 };
 
 struct gsparc_tensor {

@@ -302,6 +302,7 @@ void destroy_lane(Lane *L) {
         if (e) cudaEventDestroy(e);
     if (L->ctx.d_flag) cudaFree(L->ctx.d_flag);
     if (L->ctx.copy_stream) cudaStreamDestroy(L->ctx.copy_stream);
+    if (L->ctx.alt_stream) cudaStreamDestroy(L->ctx.alt_stream);
 }
 
 void stop_server(gsparc_server *S) {
@@ -364,6 +365,7 @@ gsparc_status gsparc_serve_create(int device, const gsparc_server_opts *opts, gs
                 GS_CUDA(cudaMalloc(&L->ctx.d_flag, 64));
                 GS_CUDA(cudaMemset(L->ctx.d_flag, 0, 64));
                 GS_CUDA(cudaStreamCreateWithFlags(&L->ctx.copy_stream, cudaStreamNonBlocking));
+                GS_CUDA(cudaStreamCreateWithFlags(&L->ctx.alt_stream, cudaStreamNonBlocking));
                 GS_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
             } catch (...) {
                 destroy_lane(L.get());
