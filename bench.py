@@ -16,6 +16,7 @@ the host->device copy of the inputs and the device->host copy of every output
 chunk (into a pinned ring) inside the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --impl reference --reference-gpu   # the reference GSPARC itself on the GPU
 
 Under torchrun each rank contracts its own instance (seed 1 + rank): weak
 scaling, no collective on the data path.
@@ -26,6 +27,7 @@ import argparse
 import json
 import math
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -57,6 +59,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work per baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-stream (batched / served) lines")
     ap.add_argument("--mixed-count", type=int, default=256, help="instances of the batched / served streams")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="with --impl reference: time the reference GSPARC program itself on the GPU, and our "
+                         "CLI on the same files, for the plain, ESC and dense-accumulator workloads")
     return ap.parse_args()
 
 
@@ -405,8 +410,92 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+REPORT_KEYS = ("Result NNZ", "SLITOM time", "Partition time", "SpTC(IdxMatch + Contraction + Data Copy) time",
+               "Total time")
+
+
+def run_report(binary, xp, yp, cx, cy, dense, iters=3, timeout=1200):
+    """Run a GSPARC-style CLI (-n iters); its stderr report as a dict (seconds per
+    iteration, averaged by the program; the last section wins)."""
+    cmd = [binary, "-X", xp, "-Y", yp, "-c", str(len(cx)), "-x", *map(str, cx), "-y", *map(str, cy),
+           "-d", str(dense), "-n", str(iters)]
+    t0 = time.perf_counter()
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout} s"}
+    out = {"rc": r.returncode, "wall_s": round(time.perf_counter() - t0, 3)}
+    for line in r.stderr.splitlines():
+        for k in REPORT_KEYS:
+            if line.startswith(k + ":"):
+                out[k] = float(line.split(":", 1)[1])
+    if r.returncode != 0:
+        out["error"] = r.stderr[-400:]
+    return out
+
+
+def host_products(X, Y, cx, cy):
+    """Matched products: per X nonzero, the number of Y nonzeros with its contract index."""
+    def lin(T, modes):
+        k = np.zeros(T.nnz, np.int64)
+        for m in modes:
+            k = k * int(T.dims[m]) + T.idx[m].astype(np.int64)
+        return k
+    xc, yc = lin(X, cx), lin(Y, cy)
+    uc, cnt = np.unique(yc, return_counts=True)
+    pos = np.minimum(np.searchsorted(uc, xc), len(uc) - 1)
+    return int(np.where(uc[pos] == xc, cnt[pos], 0).sum())
+
+
+def reference_gpu(args):
+    """The reference GSPARC program (oracle/_ref/gsparc: its main.cu and src/ compiled
+    unmodified for sm_100a) and our CLI, each run once on the same .tns files in
+    ESC mode (-d -1; ours also in its default mode), timed by their own reports."""
+    from gsparc_b200 import synth
+    import gsparc_b200 as gb
+    ref = os.path.join(ROOT, "oracle", "_ref", "gsparc")
+    if not os.path.exists(ref):
+        print(json.dumps({"impl": "reference", "reference_gpu": {"unavailable": "oracle/_ref/gsparc not built"}}))
+        return
+    cases = [("plain_small", synth.plain_small), ("esc_large", synth.esc_large), ("dense_acc", synth.dense_acc)]
+    res = {}
+    clk = Clocks(0)
+    clk.start()
+    for name, make in cases:
+        X, Y, cx, cy = make(scale=args.scale)
+        d = tempfile.mkdtemp(prefix="gsparc_refgpu_")
+        xp = os.path.join(d, "x.tns")
+        gb.write_tns(xp, X.idx, X.val)
+        yp = xp
+        if Y is not X:
+            yp = os.path.join(d, "y.tns")
+            gb.write_tns(yp, Y.idx, Y.val)
+        ir = host_products(X, Y, cx, cy)
+        row = {"nnz_x": X.nnz, "nnz_y": Y.nnz, "products": ir,
+               "reference_esc": run_report(ref, xp, yp, cx, cy, -1),
+               "ours_esc": run_report(gb.CLI_PATH, xp, yp, cx, cy, -1),
+               "ours_auto": run_report(gb.CLI_PATH, xp, yp, cx, cy, 0)}
+        for k in ("reference_esc", "ours_esc", "ours_auto"):
+            t = row[k].get("SpTC(IdxMatch + Contraction + Data Copy) time")
+            if t:
+                row[k]["products_per_s_sptc"] = ir / t
+        res[name] = row
+        print(json.dumps({name: row}), file=sys.stderr, flush=True)
+        shutil.rmtree(d, ignore_errors=True)
+    line = {"impl": "reference", "reference_gpu": {
+        "binary": "oracle/_ref/gsparc: the reference main.cu + src/, unmodified, nvcc -gencode sm_100a",
+        "timing": "each program's own stderr report (seconds per iteration, -n 3 averaged by the program, "
+                  "device memory pools set up before the first iteration in both); ours without -o drops Z "
+                  "in HBM, the reference copies every partition's Z to pinned host memory",
+        "scale": args.scale, "workloads": res}, "clocks": clk.stop()}
+    print(json.dumps(line), flush=True)
+
+
 def reference_arm(args, world, rank):
     if rank != 0:
+        return
+    if args.reference_gpu:
+        reference_gpu(args)
         return
     X, _, cx, cy = workload(0, args.scale)
     base = CpuBaseline(X, target_seconds=min(args.cpu_seconds, 8.0))

@@ -79,7 +79,7 @@ class Stats(ctypes.Structure):
 _lib = None
 
 EXPORTS = [
-    "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create",
+    "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create", "gsparc_ctx_reserve", "gsparc_host_pin", "gsparc_host_unpin",
     "gsparc_ctx_destroy", "gsparc_ctx_memory", "gsparc_tensor_upload", "gsparc_tensor_free",
     "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
     "gsparc_free_host", "gsparc_layout", "gsparc_plan_shards", "gsparc_linearize",
@@ -153,6 +153,9 @@ def lib():
     L.gsparc_status_string.argtypes = [I]
     L.gsparc_last_error.restype = ctypes.c_char_p
     L.gsparc_ctx_create.argtypes = [I, U64, ctypes.POINTER(P)]
+    L.gsparc_ctx_reserve.argtypes = [P, U64]
+    L.gsparc_host_pin.argtypes = [P, U64]
+    L.gsparc_host_unpin.argtypes = [P]
     L.gsparc_ctx_destroy.argtypes = [P]
     L.gsparc_ctx_memory.argtypes = [P, P, P, P]
     L.gsparc_tensor_upload.argtypes = [P, ctypes.POINTER(_Coo), P, ctypes.POINTER(P)]
@@ -286,6 +289,11 @@ class Context:
     @property
     def handle(self):
         return self._h
+
+    def reserve(self, nbytes: int = 0):
+        """Map nbytes (0 = the whole budget) into the context's pool now, so later
+        contractions do not grow the pool inside their stages."""
+        _check(lib().gsparc_ctx_reserve(self._h, nbytes), "ctx_reserve")
 
     def memory(self):
         a = np.zeros(3, np.uint64)

@@ -108,6 +108,42 @@ gsparc_status gsparc_ctx_destroy(gsparc_ctx *ctx) {
     });
 }
 
+gsparc_status gsparc_host_pin(void *p, uint64_t bytes) {
+    return guard([&] {
+        GS_REQUIRE(p || bytes == 0, GSPARC_EINVAL, "null buffer");
+        if (bytes) GS_CUDA(cudaHostRegister(p, bytes, cudaHostRegisterDefault));
+    });
+}
+
+gsparc_status gsparc_host_unpin(void *p) {
+    return guard([&] {
+        GS_REQUIRE(p, GSPARC_EINVAL, "null buffer");
+        GS_CUDA(cudaHostUnregister(p));
+    });
+}
+
+gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        DeviceScope ds(ctx->device);
+        uint64_t n = bytes ? std::min<uint64_t>(bytes, ctx->arena.budget()) : ctx->arena.budget();
+        n &= ~((uint64_t(1) << 21) - 1);  // whole 2 MiB pages
+        if (n == 0) return;
+        // one allocation the size of the reservation, freed at once: the pool
+        // keeps the mapped memory (its release threshold is unbounded)
+        cudaStream_t s = ctx->copy_stream;
+        void *p = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, n, ctx->arena.pool(), s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            gs::fail(e == cudaErrorMemoryAllocation ? GSPARC_ENOMEM : GSPARC_ECUDA,
+                     std::string("reserving ") + std::to_string(n) + " B failed: " + cudaGetErrorString(e));
+        }
+        GS_CUDA(cudaFreeAsync(p, s));
+        GS_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 gsparc_status gsparc_ctx_memory(gsparc_ctx *ctx, uint64_t *in_use, uint64_t *peak, uint64_t *budget) {
     return guard([&] {
         GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");

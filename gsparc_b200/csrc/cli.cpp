@@ -142,10 +142,11 @@ int run_multi(const Opts &o, const Tensor &tx, const Tensor &ty) {
     int z1o = 0;
     uint64_t z1d[32] = {};
     std::vector<int> cz1(o.na);
+    gsparc_ctx *ctx = nullptr;
+    gsparc_status s = gsparc_ctx_create(0, 0, &ctx);
+    if (!s) s = gsparc_ctx_reserve(ctx, 0);
+    if (s) die("context", s);
     for (int it = 0; it < o.iters; ++it) {
-        gsparc_ctx *ctx = nullptr;
-        gsparc_status s = gsparc_ctx_create(0, 0, &ctx);
-        if (s) die("context", s);
         const uint64_t *ix[32], *iy[32];
         for (int m = 0; m < tx.order; ++m) ix[m] = tx.idx + (size_t)m * tx.nnz;
         for (int m = 0; m < ty.order; ++m) iy[m] = ty.idx + (size_t)m * ty.nnz;
@@ -186,8 +187,8 @@ int run_multi(const Opts &o, const Tensor &tx, const Tensor &ty) {
         gsparc_tensor_free(ctx, Z1);
         gsparc_tensor_free(ctx, X);
         gsparc_tensor_free(ctx, Y);
-        gsparc_ctx_destroy(ctx);
     }
+    gsparc_ctx_destroy(ctx);
     std::fprintf(stderr, "First SpTC time: %f\n", first / o.iters);
     print_report(slitom, idxmatch, contraction, dprtn, result_nnz, o.iters);
     if (!o.out.empty()) write_output(o.out, out, z1o, z1d, cz1.data(), ty.order, ty.dims, o.cz.data(), o.na);
@@ -286,12 +287,22 @@ int main(int argc, char **argv) {
     if (st) die("reading X", st);
     st = rd(o.Y.c_str(), 0, &ty.order, ty.dims, &ty.nnz, &ty.idx, &ty.val);
     if (st) die("reading Y", st);
+    // page-locked operands upload at the full host-link rate (not timed, like
+    // the reference's cudaHostAlloc of its converted operands); unpinned
+    // memory still works if the host refuses to lock it
+    void *const bufs[4] = {tx.idx, tx.val, ty.idx, ty.val};
+    const uint64_t lens[4] = {8ull * tx.order * tx.nnz, 4ull * tx.nnz, 8ull * ty.order * ty.nnz, 4ull * ty.nnz};
+    bool pinned[4];
+    for (int i = 0; i < 4; ++i) pinned[i] = lens[i] && gsparc_host_pin(bufs[i], lens[i]) == GSPARC_OK;
+    auto release = [&] {
+        for (int i = 0; i < 4; ++i) {
+            if (pinned[i]) gsparc_host_unpin(bufs[i]);
+            gsparc_free_host(bufs[i]);
+        }
+    };
     if (o.multi) {
         const int rc = run_multi(o, tx, ty);
-        gsparc_free_host(tx.idx);
-        gsparc_free_host(tx.val);
-        gsparc_free_host(ty.idx);
-        gsparc_free_host(ty.val);
+        release();
         return rc;
     }
 
@@ -299,15 +310,34 @@ int main(int argc, char **argv) {
     uint64_t result_nnz = 0;
     OutCollect out;
 
+    // One context per GPU for the whole run, its pool mapped before any stage
+    // is timed (the reference builds its memory pools once, main.cu:56-66).
+    std::vector<gsparc_ctx *> ctxs(o.gpus, nullptr);
+    {
+        std::vector<gsparc_status> cst(o.gpus, GSPARC_OK);
+        std::vector<std::thread> th;
+        for (int g = 0; g < o.gpus; ++g)
+            th.emplace_back([&, g] {
+                cst[g] = gsparc_ctx_create(g, 0, &ctxs[g]);
+                if (!cst[g]) cst[g] = gsparc_ctx_reserve(ctxs[g], 0);
+            });
+        for (auto &t : th) t.join();
+        for (int g = 0; g < o.gpus; ++g)
+            if (cst[g]) {
+                for (auto c : ctxs)
+                    if (c) gsparc_ctx_destroy(c);
+                die("creating the device context", cst[g]);
+            }
+    }
+
     for (int it = 0; it < o.iters; ++it) {
         std::vector<gsparc_stats> stats(o.gpus);
         std::vector<gsparc_status> sts(o.gpus, GSPARC_OK);
         std::vector<double> upload_ms(o.gpus, 0.0);
         std::vector<OutCollect> parts(o.gpus);
         auto run = [&](int g) {
-            gsparc_ctx *ctx = nullptr;
-            gsparc_status s = gsparc_ctx_create(g, 0, &ctx);
-            if (s) { sts[g] = s; return; }
+            gsparc_ctx *ctx = ctxs[g];
+            gsparc_status s = GSPARC_OK;
             const uint64_t *ix[32], *iy[32];
             for (int m = 0; m < tx.order; ++m) ix[m] = tx.idx + (size_t)m * tx.nnz;
             for (int m = 0; m < ty.order; ++m) iy[m] = ty.idx + (size_t)m * ty.nnz;
@@ -351,14 +381,16 @@ int main(int argc, char **argv) {
             }
             if (X) gsparc_tensor_free(ctx, X);
             if (Y) gsparc_tensor_free(ctx, Y);
-            gsparc_ctx_destroy(ctx);
             sts[g] = s;
         };
         std::vector<std::thread> th;
         for (int g = 0; g < o.gpus; ++g) th.emplace_back(run, g);
         for (auto &t : th) t.join();
         for (int g = 0; g < o.gpus; ++g)
-            if (sts[g]) die("contraction", sts[g]);
+            if (sts[g]) {
+                for (auto c : ctxs) gsparc_ctx_destroy(c);
+                die("contraction", sts[g]);
+            }
         for (int g = 0; g < o.gpus; ++g) {
             const gsparc_stats &s = stats[g];
             if (s.accumulator == GSPARC_ACCUM_DENSE) std::fprintf(stderr, "Dense Accumulator\n");
@@ -378,11 +410,10 @@ int main(int argc, char **argv) {
         }
     }
 
+    for (auto c : ctxs) gsparc_ctx_destroy(c);
+    for (auto c : ctxs) gsparc_ctx_destroy(c);
     print_report(slitom, idxmatch, contraction, dprtn, result_nnz, o.iters);
     if (!o.out.empty()) write_output(o.out, out, tx.order, tx.dims, o.cx.data(), ty.order, ty.dims, o.cy.data(), o.nc);
-    gsparc_free_host(tx.idx);
-    gsparc_free_host(tx.val);
-    gsparc_free_host(ty.idx);
-    gsparc_free_host(ty.val);
+    release();
     return 0;
 }

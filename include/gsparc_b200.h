@@ -124,6 +124,13 @@ const char *gsparc_last_error(void);
  * allocations up to hbm_budget_bytes (0 = 90% of the device's free memory). */
 gsparc_status gsparc_ctx_create(int device, uint64_t hbm_budget_bytes, gsparc_ctx **out);
 gsparc_status gsparc_ctx_destroy(gsparc_ctx *ctx);
+/* Map `bytes` of device memory (0 = the whole budget) into the context's pool
+ * now and keep it there, so later contractions draw on memory that is already
+ * mapped instead of growing the pool inside their own stages.  The reference
+ * does the same once per run when its CudaMemoryPool takes all free HBM
+ * (src/gsparc/cuda_memory.cpp:17-28), before any stage is timed.  Admission
+ * against the budget is unchanged. */
+gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes);
 /* Bytes currently allocated by the context and its high-water mark. */
 gsparc_status gsparc_ctx_memory(gsparc_ctx *ctx, uint64_t *in_use, uint64_t *peak,
                                 uint64_t *budget);
@@ -353,6 +360,12 @@ gsparc_status gsparc_read_quantum(const char *dir, int nthreads, int *order, uin
 gsparc_status gsparc_write_tns(const char *path, int order, uint64_t nnz,
                                const uint64_t *idx /* SoA idx[m*nnz+k] */, const float *val);
 void gsparc_free_host(void *p);
+/* Page-lock an existing host buffer in place (gsparc_host_unpin releases it),
+ * so uploads from it run at the full host-link rate.  The reference keeps its
+ * converted operands in page-locked memory (cudaHostAlloc in
+ * include/gsparc/tensor_manager.tpp:223-224); the CLI pins what it read. */
+gsparc_status gsparc_host_pin(void *p, uint64_t bytes);
+gsparc_status gsparc_host_unpin(void *p);
 
 /* Bit layout of one operand.  Replaces TensorManager::compute_nbtis,
  * setup_slitom and create_mask (include/gsparc/tensor_manager.tpp:91-210):

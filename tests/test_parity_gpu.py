@@ -192,3 +192,17 @@ def test_same_result_alone_and_after_other_work(ctx):
     b = run(ctx, X, Y, cx, cy)
     assert np.array_equal(a.keys, b.keys)
     assert np.allclose(a.vals, b.vals, rtol=1e-6, atol=0)
+
+
+def test_reserved_pool_gives_the_same_result(ctx):
+    """gsparc_ctx_reserve maps the budget up front; results do not change."""
+    X, Y, cx, cy = synth.esc_large(scale=0.01)
+    a = run(ctx, X, Y, cx, cy)
+    with gb.Context(0, hbm_budget=4 << 30) as c2:
+        c2.reserve()
+        assert c2.memory()["in_use"] == 0
+        b = run(c2, X, Y, cx, cy)
+        c2.reserve(1 << 30)  # again, smaller: nothing changes
+        c = run(c2, X, Y, cx, cy)
+    assert np.array_equal(a.keys, b.keys) and np.array_equal(a.vals, b.vals)
+    assert np.array_equal(a.keys, c.keys) and np.array_equal(a.vals, c.vals)
