@@ -10,9 +10,12 @@
 // rounds back to p), so the result is bit-identical to the general paths.
 //
 // The products of all such rows of a chunk form one flat index space.  A CTA
-// takes a tile of kStreamTile consecutive products, stages the product prefix
-// of the rows that the tile touches in shared memory, and every thread maps
-// its products to (row, offset) there.  Reads of the Y run and writes of the
+// takes a tile of kStreamTile consecutive products and stages, for the rows
+// the tile touches (at most kRowBatch at a time), their flat start, first Y
+// entry, X value, output slot and key prefix in shared memory; every thread
+// then maps its products to (row, offset) there, so an output costs two
+// dependent loads (the Y entry's column rank, then its column), with SU
+// outputs' loads in flight per thread.  Reads of the Y run and writes of the
 // output are coalesced; the column table is read in ascending rank order.
 #include "blockops.cuh"
 #include "kernels.cuh"
@@ -36,8 +39,16 @@ __device__ __forceinline__ uint64_t upper_bound_u64(const uint64_t *a, uint64_t 
     return lo;
 }
 
+constexpr int kRowBatch = 512;  // rows whose parameters are staged at once
+constexpr int SU = 4;           // outputs per thread with loads in flight
+
 __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
-    __shared__ uint64_t s_pre[kStreamTile + 2];
+    __shared__ uint64_t s_pre[kRowBatch + 1];  // flat start of every staged row (+ the end)
+    __shared__ uint64_t s_xf[kRowBatch];       // x_f << Y_nfbits
+    __shared__ uint64_t s_o0[kRowBatch];       // row's first slot in the chunk buffer
+    __shared__ const uint64_t *s_cols[kRowBatch];
+    __shared__ uint32_t s_j0[kRowBatch];       // row's first Y entry
+    __shared__ float s_xv[kRowBatch];          // the row's X value
     __shared__ uint64_t s_k[2];
     const int tid = threadIdx.x;
     const uint64_t ns = a.nunits;
@@ -50,36 +61,66 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
         if (tid < 2) s_k[tid] = upper_bound_u64(a.sprefix, 0, ns + 1, P0 + (tid ? t1 - 1 : t0)) - 1;
         __syncthreads();
         const uint64_t k0 = s_k[0], k1 = s_k[1];
-        const uint32_t nk = (uint32_t)(k1 - k0 + 2);  // prefix entries k0 .. k1+1 (<= tile + 1)
-        for (uint32_t i = tid; i < nk; i += ST) s_pre[i] = a.sprefix[k0 + i] - P0;
-        __syncthreads();
-        for (uint64_t t = t0 + tid; t < t1; t += ST) {
-            uint32_t lo = 0, hi = nk - 1;  // largest i with s_pre[i] <= t
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (s_pre[mid] <= t)
-                    lo = mid;
-                else
-                    hi = mid;
+        for (uint64_t kb = k0; kb <= k1; kb += kRowBatch) {
+            const uint32_t nb = (uint32_t)(k1 - kb + 1 < (uint64_t)kRowBatch ? k1 - kb + 1 : (uint64_t)kRowBatch);
+            for (uint32_t i = tid; i <= nb; i += ST) s_pre[i] = a.sprefix[kb + i] - P0;
+            for (uint32_t i = tid; i < nb; i += ST) {
+                const uint32_t row = a.units[kb + i];
+                const uint32_t xi = a.row_xi[row];
+                int y_nfbits;
+                const uint64_t *cols;
+                uint32_t ncols;
+                row_job_params(a, row, y_nfbits, cols, ncols);
+                s_xf[i] = shl(a.row_xf[row], y_nfbits);
+                s_o0[i] = a.row_off[row] - a.chunk_base;
+                s_cols[i] = cols;
+                s_j0[i] = a.pos[xi];
+                s_xv[i] = a.xval[xi];
             }
-            const uint64_t k = k0 + lo;
-            const uint32_t p = (uint32_t)(t - s_pre[lo]);
-            const uint32_t row = a.units[k];
-            const uint32_t xi = a.row_xi[row];
-            int y_nfbits;
-            const uint64_t *cols;
-            uint32_t ncols;
-            row_job_params(a, row, y_nfbits, cols, ncols);
-            const uint32_t j = a.pos[xi] + p;
-            const uint64_t o = a.row_off[row] - a.chunk_base + p;
-            if (o < a.out_cap) {
-                __stcs(a.out_keys + o, (unsigned long long)(shl(a.row_xf[row], y_nfbits) | cols[a.yrank[j]]));
-                __stcs(a.out_vals + o, a.xval[xi] * a.yval[j]);
-            } else {
-                atomicOr(a.err, 4u);
+            __syncthreads();
+            const uint64_t b0 = t0 > s_pre[0] ? t0 : s_pre[0];
+            const uint64_t b1 = t1 < s_pre[nb] ? t1 : s_pre[nb];
+            for (uint64_t tb = b0 + tid; tb < b1; tb += (uint64_t)ST * SU) {
+                uint32_t li[SU], pp[SU], r[SU];
+                float yv[SU];
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const uint64_t t = tb + (uint64_t)u * ST;
+                    li[u] = 0;
+                    pp[u] = 0;
+                    if (t < b1) {
+                        uint32_t lo = 0, hi = nb;  // largest i with s_pre[i] <= t
+                        while (hi - lo > 1) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            if (s_pre[mid] <= t)
+                                lo = mid;
+                            else
+                                hi = mid;
+                        }
+                        li[u] = lo;
+                        pp[u] = (uint32_t)(t - s_pre[lo]);
+                        const uint32_t j = s_j0[lo] + pp[u];
+                        r[u] = a.yrank[j];
+                        yv[u] = a.yval[j];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < SU; ++u) {
+                    const uint64_t t = tb + (uint64_t)u * ST;
+                    if (t < b1) {
+                        const uint32_t i = li[u];
+                        const uint64_t o = s_o0[i] + pp[u];
+                        if (o < a.out_cap) {
+                            __stcs(a.out_keys + o, (unsigned long long)(s_xf[i] | s_cols[i][r[u]]));
+                            __stcs(a.out_vals + o, s_xv[i] * yv[u]);
+                        } else {
+                            atomicOr(a.err, 4u);
+                        }
+                    }
+                }
             }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
