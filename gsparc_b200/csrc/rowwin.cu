@@ -21,9 +21,10 @@
 //  4. (numeric) a slot -> column table is built from the bitmap (a thread per
 //     word), then every warp writes 32 consecutive slots per step.
 //
-// The window width adapts to the row's density so a window holds at most
-// kHeavyCap outputs; a window that overflows is cut at the kHeavyCap-th
-// touched column and the rest is taken by the next window.  The symbolic pass
+// The window width adapts to the row's density: each window aims at three
+// quarters of kHeavyCap outputs at the density of the window before it (at
+// most 4x wider per window); a window that overflows is cut at the
+// kHeavyCap-th touched column and the rest is taken by the next window.  The symbolic pass
 // (steps A, B, 1, 2 with the widest window) counts each row's outputs.
 #include "blockops.cuh"
 #include "kernels.cuh"
@@ -451,12 +452,17 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
             out_pos += outputs;
             row_total += outputs;
+            // next width: three quarters of the cap at the density just seen
+            // (at most 4x wider per window)
             if (over) {
-                rw = max(32u, (R1 - R0 + 31u) & ~31u);
+                rw = max(32u, ((R1 - R0) / 4u * 3u + 31u) & ~31u);
                 __syncthreads();
                 R0 = R1;
             } else {
-                if (Dw < (uint32_t)CAP / 4) rw = min((uint32_t)RW, rw * 2u);
+                const uint64_t want = Dw ? (uint64_t)rw * (uint64_t)(3 * CAP / 4) / Dw : (uint64_t)rw * 4u;
+                uint64_t nr = want < (uint64_t)rw * 4u ? want : (uint64_t)rw * 4u;
+                nr = nr > (uint64_t)RW ? (uint64_t)RW : (nr < 32u ? 32u : nr);
+                rw = (uint32_t)nr & ~31u;
                 R0 = block_min_u32<T>(nextmin, s_tmp);
             }
         }
