@@ -21,11 +21,12 @@
 //  4. (numeric) a slot -> column table is built from the bitmap (a thread per
 //     word), then every warp writes 32 consecutive slots per step.
 //
-// The window width adapts to the row's density: each window aims at three
-// quarters of kHeavyCap outputs at the density of the window before it (at
+// The window width adapts to the row's density: each window aims at fifteen
+// sixteenths of kHeavyCap outputs at the density of the window before it (at
 // most 4x wider per window); a window that overflows is cut at the
-// kHeavyCap-th touched column and the rest is taken by the next window.  The symbolic pass
-// (steps A, B, 1, 2 with the widest window) counts each row's outputs.
+// kHeavyCap-th touched column and the rest is taken by the next window.  The
+// symbolic pass (steps A, B, 1 and a popcount, on RW_SYM-wide windows: it keeps
+// neither accumulators nor the word prefix) counts each row's outputs.
 #include "blockops.cuh"
 #include "kernels.cuh"
 
@@ -42,6 +43,8 @@ constexpr int CAP = kHeavyCap;
 constexpr int MAXR = kHeavyMaxRuns;
 constexpr int WPN = (NWORDS > CAP ? NWORDS : CAP) + 4;  // word prefix, later the slot -> column table
 constexpr int WPT_MAX = (NWORDS + T - 1) / T;
+constexpr int RW_SYM = 262144;              // symbolic windows: no accumulators or word prefix kept
+constexpr int NWORDS_SYM = RW_SYM / 32;
 constexpr uint32_t INF = 0xffffffffu;
 constexpr uint32_t FULL = 0xffffffffu;
 static_assert(MAXR <= 2 * T, "run batch is scanned two per thread");
@@ -222,9 +225,10 @@ struct ProdItem {
 template <bool NUMERIC>
 __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint32_t *bits = reinterpret_cast<uint32_t *>(smem_raw);  // [NWORDS]
-    uint32_t *wp = bits + NWORDS;                              // [WPN]
-    uint32_t *seg_start = wp + WPN;                            // [MAXR]
+    constexpr int NWK = NUMERIC ? NWORDS : NWORDS_SYM;
+    uint32_t *bits = reinterpret_cast<uint32_t *>(smem_raw);  // [NWK]
+    uint32_t *wp = bits + NWK;                                 // [WPN] (numeric)
+    uint32_t *seg_start = wp + (NUMERIC ? WPN : 0);            // [MAXR]
     uint32_t *seg_off = seg_start + MAXR;                      // [MAXR + 4]
     uint32_t *seg_run = seg_off + MAXR + 4;                    // [MAXR]
     uint32_t *seg_cut = seg_run + MAXR;                        // [MAXR]
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
 
-    for (int i = tid; i < NWORDS; i += T) bits[i] = 0;
+    for (int i = tid; i < NWK; i += T) bits[i] = 0;
     if (NUMERIC)
         for (int i = tid; i < CAP; i += T) hi[i] = lo[i] = 0.f;
     __syncthreads();
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         uint32_t R0 = block_min_u32<T>(mymin, s_tmp);
 
         // initial window width from the row's density (products vs columns)
-        uint32_t rw = RW;
+        uint32_t rw = NUMERIC ? RW : RW_SYM;
         if (NUMERIC) {
             const uint64_t P = a.xprefix[xe] - a.xprefix[xs];
             const uint64_t est = (uint64_t)CAP * ncols / (P ? P : 1);
@@ -340,10 +344,11 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
             uint32_t Dw;
             uint32_t run = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
-            for (uint32_t w = w0; w < w1; ++w) {
-                wp[w] = run;
-                run += __popc(bits[w]);
-            }
+            if (NUMERIC)
+                for (uint32_t w = w0; w < w1; ++w) {
+                    wp[w] = run;
+                    run += __popc(bits[w]);
+                }
 
             if (!NUMERIC) {
                 row_total += Dw;
@@ -452,14 +457,14 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
             out_pos += outputs;
             row_total += outputs;
-            // next width: three quarters of the cap at the density just seen
+            // next width: fifteen sixteenths of the cap at the density just seen
             // (at most 4x wider per window)
             if (over) {
-                rw = max(32u, ((R1 - R0) / 4u * 3u + 31u) & ~31u);
+                rw = max(32u, ((R1 - R0) / 16u * 15u + 31u) & ~31u);
                 __syncthreads();
                 R0 = R1;
             } else {
-                const uint64_t want = Dw ? (uint64_t)rw * (uint64_t)(3 * CAP / 4) / Dw : (uint64_t)rw * 4u;
+                const uint64_t want = Dw ? (uint64_t)rw * (uint64_t)(15 * CAP / 16) / Dw : (uint64_t)rw * 4u;
                 uint64_t nr = want < (uint64_t)rw * 4u ? want : (uint64_t)rw * 4u;
                 nr = nr > (uint64_t)RW ? (uint64_t)RW : (nr < 32u ? 32u : nr);
                 rw = (uint32_t)nr & ~31u;
@@ -472,7 +477,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
 }
 
 size_t rowwin_smem(bool numeric) {
-    const size_t words = (size_t)NWORDS + WPN + MAXR + (MAXR + 4) + MAXR + MAXR;
+    const size_t words = (numeric ? (size_t)NWORDS + WPN : (size_t)NWORDS_SYM) + MAXR + (MAXR + 4) + MAXR + MAXR;
     return words * 4 + (numeric ? (size_t)CAP * 8 : 0);
 }
 
