@@ -44,7 +44,7 @@ METRIC = "matched products/sec"
 UNIT = "products/s"
 # ncu DRAM bytes (read + write) of the numeric launches (k_light<1>, k_rowwin<1>, k_stream) per output
 # nonzero, measured on esc_large at scale 0.1 (one output chunk, 2.50e8 outputs)
-TRAFFIC_BYTES_PER_OUTPUT = (27.8e6 + 2849.5e6) / 2.50473870e8
+TRAFFIC_BYTES_PER_OUTPUT = (28.42e6 + 2848.87e6) / 2.50473870e8
 
 
 def parse():
