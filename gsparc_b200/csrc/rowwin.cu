@@ -25,8 +25,9 @@
 // sixteenths of kHeavyCap outputs at the density of the window before it (at
 // most 4x wider per window); a window that overflows is cut at the
 // kHeavyCap-th touched column and the rest is taken by the next window.  The
-// symbolic pass (steps A, B, 1 and a popcount, on RW_SYM-wide windows: it keeps
-// neither accumulators nor the word prefix) counts each row's outputs.
+// symbolic pass (steps A, B and 1 on RW_SYM-wide windows: it keeps neither
+// accumulators nor the word prefix) counts each row's outputs as the columns
+// whose bit it set first.
 #include "blockops.cuh"
 #include "kernels.cuh"
 
@@ -285,6 +286,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             const uint32_t nwu = rw >> 5;  // bitmap words in use
             uint32_t nextmin = INF;
             uint32_t ns = 0;
+            uint32_t newcols = 0;  // symbolic: columns this thread marked first
 
             // ---- A, B, 1: parts of every run inside the window, marked in the bitmap
             for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
@@ -330,7 +332,10 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                     [&](uint32_t, uint32_t, const RankItem &it) {
                         const uint32_t c = it.r - R0;
                         const uint32_t m = 1u << (c & 31);
-                        if (!(bits[c >> 5] & m)) atomicOr(&bits[c >> 5], m);
+                        if (!(bits[c >> 5] & m)) {
+                            const uint32_t old = atomicOr(&bits[c >> 5], m);
+                            if (!NUMERIC) newcols += (old & m) ? 0u : 1u;
+                        }
                     });
                 __syncthreads();
             }
@@ -341,7 +346,10 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             const uint32_t w0 = (uint32_t)tid * wpt;
             const uint32_t w1 = min(w0 + wpt, nwu);
             uint32_t loc = 0;
-            for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
+            if (NUMERIC)
+                for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
+            else
+                loc = newcols;
             uint32_t Dw;
             uint32_t run = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
             if (NUMERIC)
