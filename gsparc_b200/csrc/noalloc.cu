@@ -1,11 +1,11 @@
 // noalloc.cu -- the index-match stage for callers that cannot allocate device
 // memory.
 //
-// Some callers cannot call cudaMalloc: code running while a stream is being
-// captured into a CUDA graph (allocation is not a capturable operation),
-// hosts that hand the GPU's memory to their own allocator and forbid other
-// allocations, or latency-critical paths that must not hit the driver's
-// allocator.  gsparc_index_match_noalloc does the same work as
+// Some callers cannot call cudaMalloc: hosts that hand the whole GPU memory to
+// their own allocator and forbid any other allocation (a runtime that carves
+// its arena at start-up and accounts every byte), and latency-critical paths
+// that must not enter the driver's allocator, which can synchronise the device
+// and take driver locks.  gsparc_index_match_noalloc does the same work as
 // gsparc_index_match, but its scratch (the run table of Y's contract keys and
 // CUB's temporary storage) lives in one file-scope __device__ array of
 // kScratchBytes that every GPU loading this library holds until the process
@@ -13,14 +13,18 @@
 //
 // The array's host-side name is only a stand-in; its device address is looked
 // up once per device with cudaGetSymbolAddress (with that device current) on
-// the first call made on that device.  Make that first call before any stream
-// capture begins.  Every call on a device shares the one array: calls whose
-// work overlaps on the GPU (different streams, or different host threads) race
-// on it and must be serialised by the caller.  No scratch content is carried
-// from one call to the next: every byte a call reads is written by that call.
+// the first call made on that device, so that first call should come before
+// any stream capture.  `stream` must belong to the current device (checked).
+// Every call on a device shares the one array: calls whose work overlaps on
+// the GPU (different streams, or different host threads) race on it and must
+// be serialised by the caller.  No scratch content is carried from one call to
+// the next: every byte a call reads is written by that call (the run count is
+// cleared first).
 #include <cub/cub.cuh>
 
+#include <exception>
 #include <mutex>
+#include <new>
 #include <string>
 
 #include "internal.h"
@@ -122,6 +126,12 @@ extern "C" gsparc_status gsparc_index_match_noalloc(uint64_t nx, const uint64_t 
                    "bit widths must be 0..64");
         GS_REQUIRE(nx < (1ull << 31) && ny < (1ull << 31), GSPARC_EINVAL, "more than 2^31 nonzeros");
         cudaStream_t s = (cudaStream_t)stream;
+        int cur_dev = -1, stream_dev = -1;
+        GS_CUDA(cudaGetDevice(&cur_dev));
+        GS_CUDA(cudaStreamGetDevice(s, &stream_dev));
+        GS_REQUIRE(stream_dev == cur_dev, GSPARC_EINVAL,
+                   "stream belongs to device " + std::to_string(stream_dev) + ", the current device is " +
+                       std::to_string(cur_dev));
 
         // scratch layout: flags[ny] | run_start[ny+1] | run_key[ny] | nruns | CUB temporary
         size_t t_sel = 0, t_scan = 0;
@@ -142,7 +152,8 @@ extern "C" gsparc_status gsparc_index_match_noalloc(uint64_t nx, const uint64_t 
             fail(GSPARC_EINVAL, "index match of " + std::to_string(nx) + " x " + std::to_string(ny) +
                                     " keys needs " + std::to_string(need) + " B of scratch; the no-allocation "
                                     "entry point holds " + std::to_string(kScratchBytes) +
-                                    " B (Y up to about 4.9 million keys)");
+                                    " B (about 13 B per Y key plus CUB temporary storage that grows "
+                                    "with X)");
 
         unsigned char *sc = static_cast<unsigned char *>(scratch_on_current_device());
         uint8_t *flag = sc + o_flag;
@@ -169,14 +180,22 @@ extern "C" gsparc_status gsparc_index_match_noalloc(uint64_t nx, const uint64_t 
         }
         GS_CUDA(cudaMemsetAsync(d_prefix, 0, 8, s));
         if (nx) GS_CUDA(cub::DeviceScan::InclusiveSum(tmp, t_scan, d_cnt, d_prefix + 1, (int)nx, s));
-        uint64_t h = 0;
-        GS_CUDA(cudaMemcpyAsync(&h, d_prefix + nx, 8, cudaMemcpyDeviceToHost, s));
-        GS_CUDA(cudaStreamSynchronize(s));
-        if (ir) *ir = h;
+        if (ir) {
+            uint64_t h = 0;
+            GS_CUDA(cudaMemcpyAsync(&h, d_prefix + nx, 8, cudaMemcpyDeviceToHost, s));
+            GS_CUDA(cudaStreamSynchronize(s));
+            *ir = h;
+        }
         set_last_error("");
         return GSPARC_OK;
     } catch (const Error &e) {
         set_last_error(e.msg);
         return e.st;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return GSPARC_ENOMEM;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return GSPARC_EINTERNAL;
     }
 }

@@ -406,20 +406,25 @@ gsparc_status gsparc_index_match(gsparc_ctx *ctx, uint64_t nx, const uint64_t *d
                                  int y_nfbits, uint64_t *d_pos, uint64_t *d_cnt,
                                  uint64_t *d_prefix, uint64_t *ir, void *stream);
 
-/* The same index match for callers that cannot allocate device memory: code
- * running while a stream is captured into a CUDA graph, hosts whose own
- * allocator owns the GPU's memory, paths that must not enter the driver's
- * allocator.  It needs no context and calls no cudaMalloc/cudaFree or other
- * allocating routine: its scratch (Y's run table and CUB's temporary storage)
- * is one 64 MiB file-scope device array that every GPU loading the library
- * holds until exit, enough for Y up to about 4.9 million keys; larger inputs
- * return GSPARC_EINVAL with the limit in gsparc_last_error().  The first call
+/* The same index match for callers that cannot allocate device memory:
+ * hosts whose own allocator owns all of the GPU's memory and forbids other
+ * allocations, and latency-critical paths that must not enter the driver's
+ * allocator (which can synchronise the device).  It needs no context and
+ * calls no cudaMalloc/cudaFree or other allocating routine: its scratch (Y's
+ * run table and CUB's temporary storage) is one 64 MiB file-scope device
+ * array that every GPU loading the library holds until exit.  A call needs
+ * about 13 bytes per Y key plus CUB temporary storage that grows with nx
+ * (Y up to roughly 4.9 million keys for small X); larger inputs return
+ * GSPARC_EINVAL with the bytes needed in gsparc_last_error().  The first call
  * on each device looks the array's address up (cudaGetSymbolAddress) with
- * that device current: make it before any stream capture.  All calls on a
- * device share the array, so calls that overlap on the GPU race and must be
- * serialised by the caller; nothing is carried over between calls.
- * No counterpart in the reference (its IndexMatch allocates from its pool,
- * include/gsparc/indexMatch.cuh:270-286). */
+ * that device current, so that first call should come before any stream
+ * capture.  `stream` must belong to the current device (GSPARC_EINVAL
+ * otherwise).  With ir == NULL the call does not wait: the total stays in
+ * d_prefix[nx]; otherwise it waits for the stream and stores the total.
+ * All calls on a device share the array, so calls that overlap on the GPU
+ * race and must be serialised by the caller; nothing is carried over between
+ * calls.  No counterpart in the reference (its IndexMatch allocates from its
+ * pool, include/gsparc/indexMatch.cuh:270-286). */
 gsparc_status gsparc_index_match_noalloc(uint64_t nx, const uint64_t *d_xkeys, int x_ncbits,
                                          uint64_t ny, const uint64_t *d_ykeys, int y_nfbits,
                                          uint64_t *d_pos, uint64_t *d_cnt, uint64_t *d_prefix,

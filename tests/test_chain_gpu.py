@@ -9,6 +9,7 @@ checked against the FP64 oracle run on the first result as the engine holds it
 |z - z64| <= 1e-5 * |z64| + 1e-7 * sum|products|.
 """
 import os
+import re
 import subprocess
 
 import numpy as np
@@ -152,6 +153,13 @@ def test_cli_chained_multi_sptc(ctx, tmp_path):
     assert r.returncode == 0, r.stderr
     assert "First SpTC time:" in r.stderr and "multi_sptc: 1" in r.stderr
     assert "# contract modes of Z (second SpTC): 2, contract modes: 1 2 \n" in r.stderr
+    # the reference's Table 4 script parses these lines with this pattern
+    # (scripts/figure/Table4.py:10): one match per run
+    table4 = (r"tensor X: .*?/([^/]+)\.tns[\s\S]*?First SpTC time: ([\d\.]+)[\s\S]*?"
+              r"Bit reordering time: ([\d\.]+)[\s\S]*?Total time: ([\d\.]+)")
+    m = re.findall(table4, r.stderr)
+    assert len(m) == 1 and m[0][0] == "x", m
+    assert re.search(r"Bit reordering ratio: [\d\.]+%\n", r.stderr)
     # the chain through the API on the .tns-read operands
     Xr, Yr = gb.read_tns(str(xp)), gb.read_tns(str(yp))
     dx, dy = ctx.upload(Xr), ctx.upload(Yr)

@@ -1,10 +1,11 @@
 """gsparc_index_match_noalloc -- the index match for callers that cannot
-allocate device memory (code recording a CUDA graph, hosts whose own allocator
-owns the GPU's memory, allocation-free paths).  Its scratch is one
+allocate device memory (hosts whose own allocator owns all of the GPU's memory,
+paths that must not enter the driver's allocator).  Its scratch is one
 library-owned device array, shared by every call, so the checks are: the same
-results as the allocating gsparc_index_match on the same keys, on two calls in
-a row and on two different inputs back to back (nothing may leak from one call
-into the next), and a clear refusal of inputs larger than that array.
+results as the allocating gsparc_index_match and as the oracle on the same
+keys, on two calls in a row and on two different inputs back to back (nothing
+may leak from one call into the next), the form that does not wait (ir NULL,
+total left in prefix[nx]), and a clear refusal of inputs larger than that array.
 
 Results are integers: compared exactly.  This file is collected last.
 """
@@ -43,7 +44,7 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
 
 
-def _call_noalloc(xk, ncx, yk, nfy):
+def _call_noalloc(xk, ncx, yk, nfy, want_total=True):
     import torch
     nx = xk.shape[0]
     pos = torch.full((nx,), -1, dtype=torch.int64, device="cuda")
@@ -51,10 +52,11 @@ def _call_noalloc(xk, ncx, yk, nfy):
     pre = torch.full((nx + 1,), -1, dtype=torch.int64, device="cuda")
     ir = np.zeros(1, np.uint64)
     st = _noalloc()(nx, xk.data_ptr(), ncx, yk.shape[0], yk.data_ptr(), nfy, pos.data_ptr(),
-                    cnt.data_ptr(), pre.data_ptr(), ir.ctypes.data, None)
+                    cnt.data_ptr(), pre.data_ptr(), ir.ctypes.data if want_total else None, None)
     assert st == 0, gb.lib().gsparc_last_error()
-    return (pos.cpu().numpy().view(np.uint64), cnt.cpu().numpy().view(np.uint64),
-            pre.cpu().numpy().view(np.uint64), int(ir[0]))
+    pre_h = pre.cpu().numpy().view(np.uint64)
+    total = int(ir[0]) if want_total else int(pre_h[nx])
+    return (pos.cpu().numpy().view(np.uint64), cnt.cpu().numpy().view(np.uint64), pre_h, total)
 
 
 def test_noalloc_index_match_equals_allocating_one_on_two_calls_in_a_row():
@@ -67,12 +69,16 @@ def test_noalloc_index_match_equals_allocating_one_on_two_calls_in_a_row():
             want_pre = pre.cpu().numpy().view(np.uint64)
             want_pos = pos.cpu().numpy().view(np.uint64)
             assert ir > 0
-            for _ in range(2):
-                got_pos, got_cnt, got_pre, got_ir = _call_noalloc(dx, ncx, dy, nfy)
-                assert got_ir == ir
+            o_pos, o_cnt, o_pre = ob.index_match(xk, ncx, yk, nfy)
+            assert np.array_equal(o_cnt, want_cnt) and np.array_equal(o_pre, want_pre)
+            hit = o_cnt > 0
+            for want_total in (True, True, False):
+                got_pos, got_cnt, got_pre, got_ir = _call_noalloc(dx, ncx, dy, nfy, want_total)
+                assert got_ir == ir == int(o_pre[-1])
                 assert np.array_equal(got_cnt, want_cnt)
                 assert np.array_equal(got_pre, want_pre)
                 assert np.array_equal(got_pos, want_pos)
+                assert np.array_equal(got_pos[hit], o_pos[hit])
 
 
 def test_noalloc_index_match_refuses_inputs_beyond_its_scratch():
