@@ -20,6 +20,12 @@ chunk (into a pinned ring) inside the timed region.
 
 Under torchrun each rank contracts its own instance (seed 1 + rank): weak
 scaling, no collective on the data path.
+
+``roofline``: the algorithmic bytes of the contraction (the ESC formula:
+operands read and packed, the match, every matched product written and read
+once, the output written once) over the contraction's CUDA-event time;
+``roofline_bytes_moved``: the bytes this engine does move (it never writes a
+product to HBM) over the numeric kernels' time.
 """
 from __future__ import annotations
 
@@ -44,7 +50,10 @@ METRIC = "matched products/sec"
 UNIT = "products/s"
 # ncu DRAM bytes (read + write) of the numeric launches (k_light<1>, k_rowwin<1>, k_stream) per output
 # nonzero, measured on esc_large at scale 0.1 (one output chunk, 2.50e8 outputs)
-TRAFFIC_BYTES_PER_OUTPUT = (28.42e6 + 2848.87e6) / 2.50473870e8
+TRAFFIC_NUMERIC_PER_OUTPUT = (28.42e6 + 2848.87e6) / 2.50473870e8
+# ncu DRAM bytes of every other kernel of a contraction (linearise, sort, match, planning, symbolic
+# pass) per operand nonzero (X + Y), same capture
+TRAFFIC_OTHER_PER_OPERAND_NNZ = 0.0
 
 
 def parse():
@@ -127,15 +136,37 @@ def load_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+def synth_module():
+    """gsparc_b200/synth.py (numpy only), loaded from its file so that the
+    reference arm never imports the package (which loads the engine library)."""
+    import importlib.util
+    name = "gsparc_b200_synth_standalone"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "gsparc_b200", "synth.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
 def workload(rank: int, scale: float):
-    from gsparc_b200 import synth
-    return synth.esc_large(scale=scale, seed=1 + rank)
+    return synth_module().esc_large(scale=scale, seed=1 + rank)
+
+
+def alg_bytes_contraction(nnz_x: int, order_x: int, nnz_y: int, order_y: int, ir: int, nnz_z: int) -> float:
+    """Algorithmic bytes of one ESC contraction: read the SoA COO operands and
+    write + read their packed (key, value) once, the X match (pos, cnt), the Y
+    segment scan, every matched product materialised once (write + read, 12 B
+    each) and the output written once."""
+    b = 0.0
+    for n, o in ((nnz_x, order_x), (nnz_y, order_y)):
+        b += n * (8.0 * o + 4.0) + 2.0 * 12.0 * n
+    return b + 16.0 * nnz_x + 8.0 * nnz_y + 24.0 * ir + 12.0 * nnz_z
 
 
 def cpu_sample(X, target_products: float, seed: int = 0):
     """Rows of X (whole output rows) whose products sum to about target, plus the
     nonzero at the largest coordinate so the sample's inferred dims match Y's."""
-    from gsparc_b200.synth import CooTensor
     fx = (X.idx[0] << np.uint64(12)) | X.idx[1]
     rows, inv = np.unique(fx, return_inverse=True)
     ck = (X.idx[2] << np.uint64(5)) | X.idx[3]
@@ -153,13 +184,14 @@ def cpu_sample(X, target_products: float, seed: int = 0):
 
 def run_sparta(xs_path, y_path, threads, timeout=600):
     """One run of the reference's CPU SpTC (baselines/Sparta ttt, mode 3).
-    Returns its own [Total time] in seconds, or None if it failed."""
+    Returns its own [Total time] in seconds, or None if it failed (retried a
+    few times)."""
     ttt = os.path.join(ROOT, "oracle", "_ref", "ttt")
     if not os.path.exists(ttt):
         return None
     env = dict(os.environ, EXPERIMENT_MODES="3")
     cmd = [ttt, "-X", xs_path, "-Y", y_path, "-m", "2", "-x", "2", "3", "-y", "2", "3", "-t", str(threads)]
-    for _ in range(10):  # the baseline binary crashes on about half of its runs here; retry
+    for _ in range(3):
         try:
             r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=timeout)
         except subprocess.TimeoutExpired:
@@ -171,21 +203,22 @@ def run_sparta(xs_path, y_path, threads, timeout=600):
 
 
 class CpuBaseline:
-    """The reference's CPU SpTC (or the oracle port) on bounded samples of the workload."""
+    """The reference's CPU SpTC (or the oracle port) on bounded samples of the workload.
+    Uses numpy and the baseline binary only: the engine library is not loaded."""
 
     def __init__(self, X, target_seconds: float):
-        import gsparc_b200 as gb
+        synth = synth_module()
         self.X = X
         # the cores this process may run on (the host may have more than the job is given)
         self.threads = len(os.sched_getaffinity(0)) or 1
         self.dir = tempfile.mkdtemp(prefix="gsparc_cpu_")
         self.y_path = os.path.join(self.dir, "y.tns")
-        gb.write_tns(self.y_path, X.idx, X.val)
+        synth.write_tns(self.y_path, X)
         # calibrate on a small sample
         self.kind = "reference"
         xs, ir = cpu_sample(X, 5e6, seed=7)
         p = os.path.join(self.dir, "xs_cal.tns")
-        gb.write_tns(p, xs.idx, xs.val)
+        synth.write_tns(p, xs)
         t = run_sparta(p, self.y_path, self.threads)
         if t is None or t <= 0:
             self.kind = "port"
@@ -194,7 +227,7 @@ class CpuBaseline:
         target = min(max(rate * target_seconds, 5e6), 2e9)
         self.xs, self.ir = cpu_sample(X, target, seed=11)
         self.xs_path = os.path.join(self.dir, "xs.tns")
-        gb.write_tns(self.xs_path, self.xs.idx, self.xs.val)
+        synth.write_tns(self.xs_path, self.xs)
         if self.kind == "port":
             self.threads = 1
 
@@ -414,11 +447,11 @@ REPORT_KEYS = ("Result NNZ", "SLITOM time", "Partition time", "SpTC(IdxMatch + C
                "Total time")
 
 
-def run_report(binary, xp, yp, cx, cy, dense, iters=3, timeout=1200):
+def run_report(binary, xp, yp, cx, cy, dense, iters=3, timeout=1200, extra=()):
     """Run a GSPARC-style CLI (-n iters); its stderr report as a dict (seconds per
     iteration, averaged by the program; the last section wins)."""
     cmd = [binary, "-X", xp, "-Y", yp, "-c", str(len(cx)), "-x", *map(str, cx), "-y", *map(str, cy),
-           "-d", str(dense), "-n", str(iters)]
+           "-d", str(dense), "-n", str(iters), *extra]
     t0 = time.perf_counter()
     try:
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
@@ -450,9 +483,13 @@ def host_products(X, Y, cx, cy):
 def reference_gpu(args):
     """The reference GSPARC program (oracle/_ref/gsparc: its main.cu and src/ compiled
     unmodified for sm_100a) and our CLI, each run once on the same .tns files in
-    ESC mode (-d -1; ours also in its default mode), timed by their own reports."""
-    from gsparc_b200 import synth
-    import gsparc_b200 as gb
+    ESC mode (-d -1; ours also in its default mode), timed by their own reports.
+    The reference copies every output partition to pinned host memory
+    (include/gsparc/contraction.cuh:554-555); ours does the same with -H (every
+    output chunk to a page-locked host ring), which is the like-for-like
+    comparison; ours without -H drops the output in HBM."""
+    synth = synth_module()
+    cli = os.path.join(ROOT, "gsparc_b200", "bin", "gsparc")
     ref = os.path.join(ROOT, "oracle", "_ref", "gsparc")
     if not os.path.exists(ref):
         print(json.dumps({"impl": "reference", "reference_gpu": {"unavailable": "oracle/_ref/gsparc not built"}}))
@@ -465,17 +502,20 @@ def reference_gpu(args):
         X, Y, cx, cy = make(scale=args.scale)
         d = tempfile.mkdtemp(prefix="gsparc_refgpu_")
         xp = os.path.join(d, "x.tns")
-        gb.write_tns(xp, X.idx, X.val)
+        synth.write_tns(xp, X)
         yp = xp
         if Y is not X:
             yp = os.path.join(d, "y.tns")
-            gb.write_tns(yp, Y.idx, Y.val)
+            synth.write_tns(yp, Y)
         ir = host_products(X, Y, cx, cy)
         row = {"nnz_x": X.nnz, "nnz_y": Y.nnz, "products": ir,
                "reference_esc": run_report(ref, xp, yp, cx, cy, -1),
-               "ours_esc": run_report(gb.CLI_PATH, xp, yp, cx, cy, -1),
-               "ours_auto": run_report(gb.CLI_PATH, xp, yp, cx, cy, 0)}
-        for k in ("reference_esc", "ours_esc", "ours_auto"):
+               "ours_esc_host_copy": run_report(cli, xp, yp, cx, cy, -1, extra=["-H"]),
+               "ours_auto_host_copy": run_report(cli, xp, yp, cx, cy, 0, extra=["-H"]),
+               "ours_esc_in_hbm": run_report(cli, xp, yp, cx, cy, -1),
+               "ours_auto_in_hbm": run_report(cli, xp, yp, cx, cy, 0)}
+        for k in ("reference_esc", "ours_esc_host_copy", "ours_auto_host_copy", "ours_esc_in_hbm",
+                  "ours_auto_in_hbm"):
             t = row[k].get("SpTC(IdxMatch + Contraction + Data Copy) time")
             if t:
                 row[k]["products_per_s_sptc"] = ir / t
@@ -485,8 +525,9 @@ def reference_gpu(args):
     line = {"impl": "reference", "reference_gpu": {
         "binary": "oracle/_ref/gsparc: the reference main.cu + src/, unmodified, nvcc -gencode sm_100a",
         "timing": "each program's own stderr report (seconds per iteration, -n 3 averaged by the program, "
-                  "device memory pools set up before the first iteration in both); ours without -o drops Z "
-                  "in HBM, the reference copies every partition's Z to pinned host memory",
+                  "device memory pools set up before the first iteration in both); the reference copies every "
+                  "output partition to pinned host memory, ours with -H copies every output chunk to a "
+                  "page-locked host ring (like for like), ours *_in_hbm drops the output in HBM",
         "scale": args.scale, "workloads": res}, "clocks": clk.stop()}
     print(json.dumps(line), flush=True)
 
@@ -498,7 +539,9 @@ def reference_arm(args, world, rank):
         reference_gpu(args)
         return
     X, _, cx, cy = workload(0, args.scale)
-    base = CpuBaseline(X, target_seconds=min(args.cpu_seconds, 8.0))
+    # a step is a bounded sample (about 2 s of the baseline's own time) so that
+    # the default --steps/--warmup run ends within a few minutes
+    base = CpuBaseline(X, target_seconds=min(args.cpu_seconds, 2.0))
     for _ in range(args.warmup):
         base.step()
     ts = [base.step() for _ in range(args.steps)]
@@ -569,23 +612,37 @@ def ours_arm(args, world, rank, local, dist):
         total_products = float(ir * args.steps)
     value = total_products / (ms / 1e3)
 
-    # roofline of the dominant kernel (numeric accumulation), from its own CUDA events
+    # roofline of the contraction (sort + match + accumulate, every kernel of a
+    # step), from the engine's own CUDA events: the algorithmic bytes of an ESC
+    # contraction over its time
     s0 = stats[-1]
-    t_num = float(np.mean([s["t_numeric_kernel_ms"] for s in stats]))
-    alg_bytes = 12.0 * s0["nnz"] + 16.0 * s0["nnz_x"] + 8.0 * s0["nnz_y"]
     peaks = load_peaks()
-    achieved = alg_bytes / (t_num / 1e3) / 1e9
-    # DRAM traffic of the numeric pass measured with ncu at scale 0.1: 11.5 B per output nonzero,
-    # almost all of it the output writes; it scales with the outputs.
-    traffic = TRAFFIC_BYTES_PER_OUTPUT * s0["nnz"] / max(1, s0["chunks"])
-    roofline = {"bound": "hbm", "kernel": "k_rowwin<numeric> + k_light<numeric> + k_stream",
+    t_step = float(np.mean([s["t_total_ms"] for s in stats]))
+    alg = alg_bytes_contraction(X.nnz, X.order, X.nnz, X.order, ir, s0["nnz"])
+    achieved = alg / (t_step / 1e3) / 1e9
+    traffic = (TRAFFIC_NUMERIC_PER_OUTPUT * s0["nnz"]
+               + TRAFFIC_OTHER_PER_OPERAND_NNZ * (s0["nnz_x"] + s0["nnz_y"]))
+    roofline = {"bound": "hbm", "kernel": "the contraction: linearise, sort, match, planning, symbolic and "
+                "numeric accumulation of every output chunk",
                 "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-                "traffic": traffic, "traffic_scope": "per numeric launch (one per output chunk), "
-                "scaled from an ncu capture of the same kernel at scale 0.1",
-                "alg_bytes_per_step": alg_bytes, "alg_bytes_per_launch": alg_bytes / max(1, s0["chunks"]),
-                "kernel_ms_per_step": t_num, "launches_per_step": s0["chunks"],
-                "products_per_s_in_kernel": s0["ir_nnz"] / (t_num / 1e3)}
+                "traffic": traffic,
+                "traffic_scope": "DRAM bytes read + written by every kernel of one contraction, from ncu "
+                                 "captures at scale 0.1 scaled per output (numeric kernels) and per operand "
+                                 "nonzero (the rest)",
+                "alg_bytes": alg,
+                "alg_formula": "sum over X, Y of nnz*(8*order+4) + 24*nnz, + 16*nnz_X + 8*nnz_Y + 24*products "
+                               "+ 12*nnz_Z",
+                "ms_per_contraction": t_step, "units": "one contraction per launch of the path"}
+    # the bytes this engine moves (it never writes a product to HBM): the output
+    # once, the X match arrays and the Y rank / value once, over the numeric kernels
+    t_num = float(np.mean([s["t_numeric_kernel_ms"] for s in stats]))
+    moved = 12.0 * s0["nnz"] + 16.0 * s0["nnz_x"] + 8.0 * s0["nnz_y"]
+    bytes_moved = {"kernel": "k_rowwin<numeric> + k_light<numeric> + k_stream",
+                   "achieved": moved / (t_num / 1e3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                   "frac": moved / (t_num / 1e3) / 1e9 / peaks["hbm_gbs"], "bytes_per_step": moved,
+                   "kernel_ms_per_step": t_num, "launches_per_step": s0["chunks"],
+                   "products_per_s_in_kernel": s0["ir_nnz"] / (t_num / 1e3)}
     launches = int(sum(s["kernel_launches"] for s in stats))
 
     # end to end through the public API: pinned host COO in, every output chunk out
@@ -656,6 +713,7 @@ def ours_arm(args, world, rank, local, dist):
                        "accumulator": "auto (dense window for heavy rows, on-chip ESC for light)",
                        "parallelism": f"{world} independent contractions (one per GPU)"},
             "roofline": roofline,
+            "roofline_bytes_moved": bytes_moved,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

@@ -36,6 +36,7 @@ struct Opts {
     int gpus = 1, iters = 1, dense = 0;
     bool quantum = false;
     int multi = 0;
+    bool host_copy = false;  // -H
     int na = 0;
     std::vector<int> cz;
     bool tune = false;
@@ -49,7 +50,8 @@ struct Opts {
 void usage(const char *argv0) {
     std::fprintf(stderr,
                  "Usage: %s -X x.tns -Y y.tns -c N -x m1..mN -y m1..mN [-g G] [-n iters] [-d 1|0|-1] [-q]\n"
-                 "          [-m 1 -a K -z t1..tK] [-t] [-o z.tns]\n",
+                 "          [-m 1 -a K -z t1..tK] [-t] [-o z.tns | -H]\n"
+                 "  -H  copy every output chunk to page-locked host memory (and drop it there)\n",
                  argv0);
 }
 
@@ -209,7 +211,7 @@ int run_multi(const Opts &o, const Tensor &tx, const Tensor &ty) {
 int main(int argc, char **argv) {
     Opts o;
     int c;
-    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhvt")) != -1) {
+    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhvtH")) != -1) {
         switch (c) {
         case 'X':
             std::fprintf(stderr, "tensor X: %s\n", optarg);
@@ -271,6 +273,9 @@ int main(int argc, char **argv) {
             break;
         case 't':
             o.tune = true;
+            break;
+        case 'H':
+            o.host_copy = true;
             break;
         case 'b':
         case 'v':
@@ -358,9 +363,31 @@ int main(int argc, char **argv) {
                 !(s = gsparc_tensor_upload(ctx, &cy, nullptr, &Y))) {
                 upload_ms[g] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
                 gsparc_sink sink{};
-                sink.kind = o.out.empty() ? GSPARC_SINK_DISCARD : GSPARC_SINK_DEVICE;
+                sink.kind = GSPARC_SINK_DISCARD;
                 std::vector<uint64_t> hk;
                 std::vector<float> hv;
+                if (o.host_copy && o.out.empty()) {
+                    // -H: every output chunk copied to a page-locked host ring and
+                    // dropped there, as the reference copies each output partition to
+                    // pinned host memory (contraction.cuh:554-555)
+                    sink.kind = GSPARC_SINK_HOST;
+                    hk.resize(1 << 26);
+                    hv.resize(1 << 26);
+                    sink.host_keys = hk.data();
+                    sink.host_vals = hv.data();
+                    sink.host_capacity = hk.size();
+                    const bool pk = gsparc_host_pin(hk.data(), 8 * hk.size()) == GSPARC_OK;
+                    const bool pv = gsparc_host_pin(hv.data(), 4 * hv.size()) == GSPARC_OK;
+                    if (!s)
+                        s = gsparc_sptc_shard(ctx, X, Y, o.nc, o.cx.data(), o.cy.data(), o.dense, g, o.gpus, &sink,
+                                              &stats[g], nullptr);
+                    if (pk) gsparc_host_unpin(hk.data());
+                    if (pv) gsparc_host_unpin(hv.data());
+                    if (X) gsparc_tensor_free(ctx, X);
+                    if (Y) gsparc_tensor_free(ctx, Y);
+                    sts[g] = s;
+                    return;
+                }
                 if (!o.out.empty()) {
                     sink.kind = GSPARC_SINK_HOST;
                     hk.resize(1 << 24);
@@ -419,7 +446,6 @@ int main(int argc, char **argv) {
         }
     }
 
-    for (auto c : ctxs) gsparc_ctx_destroy(c);
     for (auto c : ctxs) gsparc_ctx_destroy(c);
     print_report(slitom, idxmatch, contraction, dprtn, result_nnz, o.iters);
     if (!o.out.empty()) write_output(o.out, out, tx.order, tx.dims, o.cx.data(), ty.order, ty.dims, o.cy.data(), o.nc);

@@ -47,3 +47,29 @@ def test_host_products_equals_the_oracle_count():
     for X, Y, cx, cy in (synth.plain_small(scale=0.05), synth.esc_large(scale=0.003),
                          synth.dense_acc(scale=0.0005)):
         assert bench.host_products(X, Y, cx, cy) == ob.sptc(X, Y, cx, cy).ir_nnz
+
+
+def test_algorithmic_bytes_of_a_contraction():
+    # X, Y of order 3 and 4 with 10 and 20 nonzeros, 100 products, 30 outputs
+    want = (10 * (8 * 3 + 4) + 24 * 10) + (20 * (8 * 4 + 4) + 24 * 20) + 16 * 10 + 8 * 20 + 24 * 100 + 12 * 30
+    assert bench.alg_bytes_contraction(10, 3, 20, 4, 100, 30) == want
+
+
+def test_reference_arm_does_not_load_the_engine_library(tmp_path):
+    """The reference arm (Sparta on a sample) runs on numpy and the baseline
+    binary only: neither the package nor its shared library is loaded."""
+    import subprocess
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import bench\n"
+        "X, _, _, _ = bench.workload(0, 0.01)\n"
+        "b = bench.CpuBaseline(X, target_seconds=0.2)\n"
+        "t = b.step()\n"
+        "assert t > 0, t\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "assert 'libgsparc_b200' not in maps\n"
+        "assert not any(m == 'gsparc_b200' or m.startswith('gsparc_b200.') for m in sys.modules)\n"
+        "print('ok', b.kind, b.ir)\n" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.startswith("ok")
