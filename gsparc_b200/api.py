@@ -70,7 +70,10 @@ class Stats(ctypes.Structure):
                 ("t_output_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
                 ("bytes_h2d", ctypes.c_uint64), ("bytes_d2h", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("t_numeric_kernel_ms", ctypes.c_double),
-                ("heavy_windows", ctypes.c_uint64), ("stream_rows", ctypes.c_uint64)]
+                ("heavy_windows", ctypes.c_uint64), ("stream_rows", ctypes.c_uint64),
+                ("verified_nnz", ctypes.c_uint64), ("verified_products", ctypes.c_uint64),
+                ("verify_mismatch", ctypes.c_uint64), ("verify_skipped_rows", ctypes.c_uint64),
+                ("max_rel_err", ctypes.c_double), ("max_abs_err", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -79,14 +82,16 @@ class Stats(ctypes.Structure):
 _lib = None
 
 EXPORTS = [
-    "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create", "gsparc_ctx_reserve", "gsparc_host_pin", "gsparc_host_unpin",
+    "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create", "gsparc_ctx_reserve",
+    "gsparc_ctx_set_verify", "gsparc_host_pin", "gsparc_host_unpin",
     "gsparc_ctx_destroy", "gsparc_ctx_memory", "gsparc_tensor_upload", "gsparc_tensor_free",
     "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
     "gsparc_free_host", "gsparc_layout", "gsparc_plan_shards", "gsparc_linearize",
     "gsparc_sort_pairs", "gsparc_index_match", "gsparc_digest_chunk", "gsparc_sptc_batch",
     "gsparc_serve_create", "gsparc_serve_destroy", "gsparc_serve_upload", "gsparc_serve_release",
     "gsparc_serve_submit", "gsparc_serve_poll", "gsparc_serve_wait", "gsparc_serve_stats",
-    "gsparc_serve_reset_stats", "gsparc_sptc_resident", "gsparc_tensor_download",
+    "gsparc_serve_reset_stats", "gsparc_serve_pause", "gsparc_serve_inject_alloc_failure",
+    "gsparc_ctx_inject_alloc_failure", "gsparc_sptc_resident", "gsparc_tensor_download",
     "gsparc_read_quantum", "gsparc_autotune", "gsparc_plan_create", "gsparc_plan_chunks", "gsparc_plan_chunk",
     "gsparc_plan_job_output", "gsparc_plan_refresh", "gsparc_plan_execute", "gsparc_plan_check",
     "gsparc_plan_destroy", "gsparc_tensor_set_values",
@@ -154,6 +159,7 @@ def lib():
     L.gsparc_last_error.restype = ctypes.c_char_p
     L.gsparc_ctx_create.argtypes = [I, U64, ctypes.POINTER(P)]
     L.gsparc_ctx_reserve.argtypes = [P, U64]
+    L.gsparc_ctx_set_verify.argtypes = [P, U64]
     L.gsparc_host_pin.argtypes = [P, U64]
     L.gsparc_host_unpin.argtypes = [P]
     L.gsparc_ctx_destroy.argtypes = [P]
@@ -196,6 +202,9 @@ def lib():
     L.gsparc_serve_wait.argtypes = [P, U64, ctypes.c_double, ctypes.POINTER(_Job)]
     L.gsparc_serve_stats.argtypes = [P, ctypes.POINTER(ServeStats)]
     L.gsparc_serve_reset_stats.argtypes = [P]
+    L.gsparc_serve_pause.argtypes = [P, I]
+    L.gsparc_serve_inject_alloc_failure.argtypes = [P, U64]
+    L.gsparc_ctx_inject_alloc_failure.argtypes = [P, U64]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype if name in (
             "gsparc_version", "gsparc_status_string", "gsparc_last_error") else (
@@ -295,6 +304,17 @@ class Context:
         contractions do not grow the pool inside their stages."""
         _check(lib().gsparc_ctx_reserve(self._h, nbytes), "ctx_reserve")
 
+    def inject_alloc_failure(self, nth: int):
+        """Host-side fault injection: the nth device allocation of this context
+        from now (1 = the next) fails with GSPARC_ENOMEM, once; 0 disarms."""
+        _check(lib().gsparc_ctx_inject_alloc_failure(self._h, nth), "ctx_inject_alloc_failure")
+
+    def set_verify(self, max_products: int):
+        """FP64 verification of later contractions' outputs on the GPU (all rows
+        up to max_products matched products, a sample of rows above; 0 = off);
+        results in the stats: max_rel_err, max_abs_err, verified_nnz, ..."""
+        _check(lib().gsparc_ctx_set_verify(self._h, max_products), "ctx_set_verify")
+
     def memory(self):
         a = np.zeros(3, np.uint64)
         _check(lib().gsparc_ctx_memory(self._h, _p(a[0:1]), _p(a[1:2]), _p(a[2:3])), "ctx_memory")
@@ -331,7 +351,7 @@ class DeviceTensor:
         self.dims = [int(d) for d in t.dims]
         self._dims = np.asarray(self.dims, np.uint64)
         on_device = 0
-        if isinstance(t, CooTensor):
+        if isinstance(t.val, np.ndarray):  # host COO (CooTensor or any object with dims/idx/val arrays)
             self._idx = np.ascontiguousarray(t.idx, np.uint64)
             self._val = np.ascontiguousarray(t.val, np.float32)
             nnz = self._val.shape[0]
@@ -797,6 +817,15 @@ class Server:
 
     def reset_stats(self) -> None:
         _check(lib().gsparc_serve_reset_stats(self._h), "serve_reset_stats")
+
+    def pause(self, paused: bool = True) -> None:
+        """Hold the lanes (no new batch starts) or resume them."""
+        _check(lib().gsparc_serve_pause(self._h, int(bool(paused))), "serve_pause")
+
+    def inject_alloc_failure(self, nth: int) -> None:
+        """Host-side fault injection: every lane's nth device allocation from
+        now fails with GSPARC_ENOMEM, once (0 disarms)."""
+        _check(lib().gsparc_serve_inject_alloc_failure(self._h, nth), "serve_inject_alloc_failure")
 
     def close(self) -> None:
         if self._h:

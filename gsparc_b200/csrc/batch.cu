@@ -27,6 +27,7 @@
 
 #include "engine.h"
 #include "kernels.cuh"
+#include "verify.h"
 #include "wide.h"
 
 namespace gs {
@@ -627,6 +628,7 @@ struct GroupPlan {
     DBuf<BLin> d_lx, d_ly;
     DBuf<uint64_t> d_xoffs, d_yoffs;
     DBuf<float> xperm, yperm, xvals, yvals;
+    DBuf<uint64_t> ykeys;  // sorted Y keys (the single-run-row copy reads y_f from them)
     DBuf<BatchJob> d_acc;
     DBuf<uint32_t> rank, pos, cnt, row_start, units, H, H2, SR, row_xi, cursor, pend;
     DBuf<uint64_t> cols, xprefix, row_xf, sprefix, row_off;
@@ -756,6 +758,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     if (wy) { yk0.release(); yv0.release(); } else { yk1.release(); yv1.release(); }
     if (keep) {
         // the sorted "values" are input positions: keep them, fetch the values
+        keep->ykeys = wy ? std::move(yk1) : std::move(yk0);  // ykeys keeps pointing at it
         keep->xperm = wx ? std::move(xv1) : std::move(xv0);
         keep->yperm = wy ? std::move(yv1) : std::move(yv0);
         keep->xvals.reset(A, std::max<uint64_t>(nx, 1), s);
@@ -942,6 +945,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     aa.xval = xvals;
     aa.yrank = rank;
     aa.yval = yvals;
+    aa.ykeys = ykeys;
     aa.cols = cols;
     aa.work_counter = ctx->d_flag + 1;
     aa.cursor = cursor;
@@ -1160,6 +1164,31 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     std::vector<cudaEvent_t> kev(2 * chunks.size(), nullptr);
     for (auto &e : kev) GS_CUDA(cudaEventCreate(&e));
     cudaStream_t s2 = ctx->copy_stream;
+
+    // FP64 verification of every chunk before delivery (off unless asked for)
+    const bool verify = ctx->verify_budget != 0 && nrows > 0 && ntot > 0;
+    VerifyState vs;
+    DBuf<VerifyEntry> v_list;
+    DBuf<unsigned long long> v_cnt;
+    DBuf<double> v_acc;
+    DBuf<VerifyOut> v_out;
+    if (verify) {
+        v_list.reset(A, nrows, s);
+        v_cnt.reset(A, 2, s);
+        v_out.reset(A, g, s);
+        GS_CUDA(cudaMemsetAsync(v_out.get(), 0, sizeof(VerifyOut) * g, s));
+        uint64_t cap = std::min<uint64_t>(bufn, 1ull << 25);
+        cap = std::max<uint64_t>(1, std::min<uint64_t>(cap, A.available() / 2 / sizeof(double)));
+        v_acc.reset(A, cap, s);
+        vs.list = v_list.get();
+        vs.cnt = v_cnt.get();
+        vs.acc = v_acc.get();
+        vs.acc_cap = cap;
+        vs.out = v_out.get();
+        vs.threshold = verify_threshold(ctx->verify_budget, ir);
+        vs.salt = 0x5eed5eed5eedull;
+        GS_CUDA(cudaStreamSynchronize(s));
+    }
     double t_out = 0;
     std::vector<uint64_t> job_first(g + 1);
     for (int j = 0; j <= g; ++j) job_first[j] = jo[j].out_off;
@@ -1212,6 +1241,11 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
         GS_CUDA(cudaStreamWaitEvent(s2, kev[2 * ci + 1], 0));
         GS_CUDA(cudaEventSynchronize(kev[2 * ci + 1]));
         const uint64_t c0 = c.first, c1 = c.first + c.n;
+        if (verify) {
+            // before any wide-key remap: the chunk still holds the engine's keys
+            verify_chunk(aa, vs, nrows, c0, c1, out_k[bi].get(), out_v[bi].get(), s2);
+            GS_CUDA(cudaStreamSynchronize(s2));  // the buffer is rewritten two chunks on
+        }
         // jobs overlapping [c0, c1)
         int j = (int)(std::upper_bound(job_first.begin(), job_first.end(), c0) - job_first.begin()) - 1;
         for (j = std::max(j, 0); j < g && job_first[j] < c1; ++j) {
@@ -1263,6 +1297,15 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     GS_CUDA(cudaStreamWaitEvent(s, ev_alt, 0));
     cudaEventDestroy(ev_ready);
     cudaEventDestroy(ev_alt);
+    if (verify) {
+        std::vector<VerifyOut> vo(g);
+        d2h(vo.data(), v_out.get(), g, s2);
+        GS_CUDA(cudaStreamSynchronize(s2));
+        for (int j = 0; j < g; ++j) {
+            verify_fill_stats(vo[j], G[j]->job->stats);
+            verify_fill_stats(vo[j], bst);
+        }
+    }
     mark(5);
     unsigned int hflags[4] = {0, 0, 0, 0};
     d2h(hflags, ctx->d_flag, 4, s);

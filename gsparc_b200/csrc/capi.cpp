@@ -122,6 +122,20 @@ gsparc_status gsparc_host_unpin(void *p) {
     });
 }
 
+gsparc_status gsparc_ctx_inject_alloc_failure(gsparc_ctx *ctx, uint64_t nth) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        ctx->arena.inject_failure(nth);
+    });
+}
+
+gsparc_status gsparc_ctx_set_verify(gsparc_ctx *ctx, uint64_t max_products) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        ctx->verify_budget = max_products;
+    });
+}
+
 gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes) {
     return guard([&] {
         GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");

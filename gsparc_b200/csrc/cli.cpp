@@ -37,6 +37,8 @@ struct Opts {
     bool quantum = false;
     int multi = 0;
     bool host_copy = false;  // -H
+    bool verify = false;     // -V
+    bool one_device = false; // -e: the -g row shards one after another on device 0
     int na = 0;
     std::vector<int> cz;
     bool tune = false;
@@ -50,8 +52,12 @@ struct Opts {
 void usage(const char *argv0) {
     std::fprintf(stderr,
                  "Usage: %s -X x.tns -Y y.tns -c N -x m1..mN -y m1..mN [-g G] [-n iters] [-d 1|0|-1] [-q]\n"
-                 "          [-m 1 -a K -z t1..tK] [-t] [-o z.tns | -H]\n"
-                 "  -H  copy every output chunk to page-locked host memory (and drop it there)\n",
+                 "          [-m 1 -a K -z t1..tK] [-t] [-o z.tns | -H] [-V] [-e]\n"
+                 "  -H  copy every output chunk to page-locked host memory (and drop it there)\n"
+                 "  -V  verify the values against FP64 sums on the GPU (all rows up to 2^28\n"
+                 "      products, a seeded sample of rows above) and print the max errors\n"
+                 "  -e  run the -g G row shards one after another on device 0 (their outputs\n"
+                 "      concatenate into the same Z as on G devices)\n",
                  argv0);
 }
 
@@ -211,7 +217,7 @@ int run_multi(const Opts &o, const Tensor &tx, const Tensor &ty) {
 int main(int argc, char **argv) {
     Opts o;
     int c;
-    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhvtH")) != -1) {
+    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhvtHVe")) != -1) {
         switch (c) {
         case 'X':
             std::fprintf(stderr, "tensor X: %s\n", optarg);
@@ -277,6 +283,12 @@ int main(int argc, char **argv) {
         case 'H':
             o.host_copy = true;
             break;
+        case 'V':
+            o.verify = true;
+            break;
+        case 'e':
+            o.one_device = true;
+            break;
         case 'b':
         case 'v':
             break;
@@ -323,20 +335,23 @@ int main(int argc, char **argv) {
     double slitom = 0, idxmatch = 0, contraction = 0, dprtn = 0;
     uint64_t result_nnz = 0;
     OutCollect out;
+    gsparc_stats vsum{};  // -V: verification of the last iteration, over all GPUs
 
     // One context per GPU for the whole run, its pool mapped before any stage
     // is timed (the reference builds its memory pools once, main.cu:56-66).
-    std::vector<gsparc_ctx *> ctxs(o.gpus, nullptr);
+    const int nctx = o.one_device ? 1 : o.gpus;
+    std::vector<gsparc_ctx *> ctxs(nctx, nullptr);
     {
-        std::vector<gsparc_status> cst(o.gpus, GSPARC_OK);
+        std::vector<gsparc_status> cst(nctx, GSPARC_OK);
         std::vector<std::thread> th;
-        for (int g = 0; g < o.gpus; ++g)
+        for (int g = 0; g < nctx; ++g)
             th.emplace_back([&, g] {
                 cst[g] = gsparc_ctx_create(g, 0, &ctxs[g]);
                 if (!cst[g]) cst[g] = gsparc_ctx_reserve(ctxs[g], 0);
+                if (!cst[g] && o.verify) cst[g] = gsparc_ctx_set_verify(ctxs[g], 1ull << 28);
             });
         for (auto &t : th) t.join();
-        for (int g = 0; g < o.gpus; ++g)
+        for (int g = 0; g < nctx; ++g)
             if (cst[g]) {
                 for (auto c : ctxs)
                     if (c) gsparc_ctx_destroy(c);
@@ -350,7 +365,7 @@ int main(int argc, char **argv) {
         std::vector<double> upload_ms(o.gpus, 0.0);
         std::vector<OutCollect> parts(o.gpus);
         auto run = [&](int g) {
-            gsparc_ctx *ctx = ctxs[g];
+            gsparc_ctx *ctx = ctxs[o.one_device ? 0 : g];
             gsparc_status s = GSPARC_OK;
             const uint64_t *ix[32], *iy[32];
             for (int m = 0; m < tx.order; ++m) ix[m] = tx.idx + (size_t)m * tx.nnz;
@@ -420,15 +435,26 @@ int main(int argc, char **argv) {
             sts[g] = s;
         };
         std::vector<std::thread> th;
-        for (int g = 0; g < o.gpus; ++g) th.emplace_back(run, g);
+        for (int g = 0; g < o.gpus; ++g) {
+            if (o.one_device)
+                run(g);
+            else
+                th.emplace_back(run, g);
+        }
         for (auto &t : th) t.join();
         for (int g = 0; g < o.gpus; ++g)
             if (sts[g]) {
                 for (auto c : ctxs) gsparc_ctx_destroy(c);
                 die("contraction", sts[g]);
             }
+        vsum = gsparc_stats{};
         for (int g = 0; g < o.gpus; ++g) {
             const gsparc_stats &s = stats[g];
+            vsum.verified_nnz += s.verified_nnz;
+            vsum.verified_products += s.verified_products;
+            vsum.verify_mismatch += s.verify_mismatch;
+            vsum.max_rel_err = std::max(vsum.max_rel_err, s.max_rel_err);
+            vsum.max_abs_err = std::max(vsum.max_abs_err, s.max_abs_err);
             if (s.accumulator == GSPARC_ACCUM_DENSE) std::fprintf(stderr, "Dense Accumulator\n");
             result_nnz += s.nnz;
             slitom += (upload_ms[g] + s.t_linearize_ms + s.t_sort_ms) / 1e3 / o.gpus;
@@ -448,6 +474,12 @@ int main(int argc, char **argv) {
 
     for (auto c : ctxs) gsparc_ctx_destroy(c);
     print_report(slitom, idxmatch, contraction, dprtn, result_nnz, o.iters);
+    if (o.verify)
+        std::fprintf(stderr,
+                     "FP64 verification: %llu outputs, %llu products, %llu mismatches, max rel err %.3e, "
+                     "max abs err %.3e\n",
+                     (unsigned long long)vsum.verified_nnz, (unsigned long long)vsum.verified_products,
+                     (unsigned long long)vsum.verify_mismatch, vsum.max_rel_err, vsum.max_abs_err);
     if (!o.out.empty()) write_output(o.out, out, tx.order, tx.dims, o.cx.data(), ty.order, ty.dims, o.cy.data(), o.nc);
     release();
     return 0;

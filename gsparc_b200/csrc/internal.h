@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <unordered_map>
@@ -77,6 +78,9 @@ public:
     uint64_t in_use() const { return in_use_; }
     uint64_t peak() const { return peak_; }
     uint64_t budget() const { return budget_; }
+    // Host-side fault injection: the nth allocation from now (1 = the next)
+    // fails with GSPARC_ENOMEM, once; 0 disarms.  Nothing touches the device.
+    void inject_failure(uint64_t nth) { fail_in_.store(nth); }
     uint64_t available() const { return budget_ > in_use_ ? budget_ - in_use_ : 0; }
     int device() const { return device_; }
     cudaMemPool_t pool() const { return pool_; }
@@ -87,6 +91,7 @@ private:
     bool owns_pool_ = false;
     uint64_t budget_ = 0, in_use_ = 0, peak_ = 0;
     std::unordered_map<void *, size_t> sizes_;
+    std::atomic<uint64_t> fail_in_{0};
 };
 
 // RAII device buffer from an Arena.
@@ -137,6 +142,7 @@ struct gsparc_ctx {
     unsigned int *d_flag = nullptr;  // device error / work counters
     cudaStream_t copy_stream = nullptr;  // output chunk copies (non-blocking)
     cudaStream_t alt_stream = nullptr;   // every other output chunk's kernels (non-blocking)
+    uint64_t verify_budget = 0;          // FP64 verification of outputs (0: off)
 };
 
 struct gsparc_tensor {

@@ -81,6 +81,7 @@ struct AccArgs {
     // Y side
     const uint32_t *yrank;
     const float *yval;
+    const uint64_t *ykeys;     // sorted Y keys (c << nfbits | y_f, job id above): y_f without the column table
     const uint64_t *cols;
     int y_nfbits;
     // single-run rows (stream path): the matched X nonzero of every such row,

@@ -93,6 +93,7 @@ struct gsparc_server {
     uint64_t reserved = 0;  // working memory admitted to running batches
     int running = 0;
     bool stop = false;
+    bool paused = false;  // gsparc_serve_pause: lanes take no new batch
 
     // statistics
     std::vector<double> lat_ms;
@@ -210,8 +211,8 @@ void lane_main(gsparc_server *S, Lane *L) {
     cudaSetDevice(S->device);
     std::unique_lock<std::mutex> lk(S->mu);
     for (;;) {
-        S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
-        if (S->queue.empty()) {
+        S->cv_work.wait(lk, [&] { return S->stop || (!S->paused && !S->queue.empty()); });
+        if (S->queue.empty() || S->paused) {
             if (S->stop) return;
             continue;
         }
@@ -565,6 +566,22 @@ gsparc_status gsparc_serve_stats(gsparc_server *srv, gsparc_server_stats *out) {
             out->wall_ms = std::chrono::duration<double, std::milli>(srv->t_last - srv->t_first).count();
             if (out->wall_ms > 0) out->products_per_s = (double)srv->ir / (out->wall_ms / 1e3);
         }
+    });
+}
+
+gsparc_status gsparc_serve_pause(gsparc_server *srv, int paused) {
+    return guard([&] {
+        GS_REQUIRE(srv, GSPARC_EINVAL, "null server");
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->paused = paused != 0;
+        srv->cv_work.notify_all();
+    });
+}
+
+gsparc_status gsparc_serve_inject_alloc_failure(gsparc_server *srv, uint64_t nth) {
+    return guard([&] {
+        GS_REQUIRE(srv, GSPARC_EINVAL, "null server");
+        for (auto &L : srv->lanes) L->ctx.arena.inject_failure(nth);
     });
 }
 

@@ -14,9 +14,9 @@
 // the tile touches (at most kRowBatch at a time), their flat start, first Y
 // entry, X value, output slot and key prefix in shared memory; every thread
 // then maps its products to (row, offset) there, so an output costs two
-// dependent loads (the Y entry's column rank, then its column), with SU
-// outputs' loads in flight per thread.  Reads of the Y run and writes of the
-// output are coalesced; the column table is read in ascending rank order.
+// coalesced loads of the Y entry (its sorted key, whose low Y_nfbits bits are
+// the output column y_f, and its value), with SU outputs' loads in flight per
+// thread, and coalesced writes of the output.
 #include "blockops.cuh"
 #include "kernels.cuh"
 
@@ -39,6 +39,8 @@ __device__ __forceinline__ uint64_t upper_bound_u64(const uint64_t *a, uint64_t 
     return lo;
 }
 
+__device__ __forceinline__ uint64_t low_mask(int b) { return b >= 64 ? ~0ull : ((1ull << b) - 1); }
+
 constexpr int kRowBatch = 512;  // rows whose parameters are staged at once
 constexpr int SU = 4;           // outputs per thread with loads in flight
 
@@ -46,7 +48,7 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
     __shared__ uint64_t s_pre[kRowBatch + 1];  // flat start of every staged row (+ the end)
     __shared__ uint64_t s_xf[kRowBatch];       // x_f << Y_nfbits
     __shared__ uint64_t s_o0[kRowBatch];       // row's first slot in the chunk buffer
-    __shared__ const uint64_t *s_cols[kRowBatch];
+    __shared__ uint64_t s_ym[kRowBatch];       // mask of the y_f bits of a Y key
     __shared__ uint32_t s_j0[kRowBatch];       // row's first Y entry
     __shared__ float s_xv[kRowBatch];          // the row's X value
     __shared__ uint64_t s_k[2];
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
                 row_job_params(a, row, y_nfbits, cols, ncols);
                 s_xf[i] = shl(a.row_xf[row], y_nfbits);
                 s_o0[i] = a.row_off[row] - a.chunk_base;
-                s_cols[i] = cols;
+                s_ym[i] = low_mask(y_nfbits);
                 s_j0[i] = a.pos[xi];
                 s_xv[i] = a.xval[xi];
             }
@@ -81,7 +83,8 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
             const uint64_t b0 = t0 > s_pre[0] ? t0 : s_pre[0];
             const uint64_t b1 = t1 < s_pre[nb] ? t1 : s_pre[nb];
             for (uint64_t tb = b0 + tid; tb < b1; tb += (uint64_t)ST * SU) {
-                uint32_t li[SU], pp[SU], r[SU];
+                uint32_t li[SU], pp[SU];
+                uint64_t yk[SU];
                 float yv[SU];
 #pragma unroll
                 for (int u = 0; u < SU; ++u) {
@@ -100,7 +103,7 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
                         li[u] = lo;
                         pp[u] = (uint32_t)(t - s_pre[lo]);
                         const uint32_t j = s_j0[lo] + pp[u];
-                        r[u] = a.yrank[j];
+                        yk[u] = a.ykeys[j];
                         yv[u] = a.yval[j];
                     }
                 }
@@ -111,7 +114,7 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
                         const uint32_t i = li[u];
                         const uint64_t o = s_o0[i] + pp[u];
                         if (o < a.out_cap) {
-                            __stcs(a.out_keys + o, (unsigned long long)(s_xf[i] | s_cols[i][r[u]]));
+                            __stcs(a.out_keys + o, (unsigned long long)(s_xf[i] | (yk[u] & s_ym[i])));
                             __stcs(a.out_vals + o, s_xv[i] * yv[u]);
                         } else {
                             atomicOr(a.err, 4u);

@@ -89,6 +89,12 @@ void Arena::init_shared(int device, cudaMemPool_t pool, uint64_t budget) {
 
 void *Arena::alloc(size_t bytes, cudaStream_t s) {
     bytes = (bytes + 255) & ~size_t(255);
+    for (uint64_t f = fail_in_.load(); f != 0;) {
+        if (fail_in_.compare_exchange_weak(f, f - 1)) {
+            if (f == 1) fail(GSPARC_ENOMEM, "injected allocation failure (" + std::to_string(bytes) + " B)");
+            break;
+        }
+    }
     if (in_use_ + bytes > budget_)
         fail(GSPARC_ENOMEM, "HBM budget exhausted: need " + std::to_string(bytes) + " B, " +
                                 std::to_string(available()) + " B left of " + std::to_string(budget_));

@@ -110,6 +110,15 @@ typedef struct {
     double t_numeric_kernel_ms; /* device time of the numeric accumulation kernels */
     uint64_t heavy_windows;   /* column windows swept by the heavy-row accumulator */
     uint64_t stream_rows;     /* rows with one matched run, copied without accumulation */
+    /* FP64 verification (gsparc_ctx_set_verify; all zero when it is off):
+     * outputs compared with the FP64 sums of their exact products, formed on
+     * the GPU.  No counterpart in the reference, which never inspects Z. */
+    uint64_t verified_nnz;      /* outputs checked                               */
+    uint64_t verified_products; /* matched products summed in FP64              */
+    uint64_t verify_mismatch;   /* products whose output key is missing, NaNs   */
+    uint64_t verify_skipped_rows; /* sampled rows past the FP64 scratch (unchecked) */
+    double max_rel_err;         /* max |z - z64| / |z64| over checked z64 != 0   */
+    double max_abs_err;         /* max |z - z64| over checked outputs            */
 } gsparc_stats;
 
 /* ---- version / errors ---------------------------------------------------- */
@@ -131,6 +140,19 @@ gsparc_status gsparc_ctx_destroy(gsparc_ctx *ctx);
  * (src/gsparc/cuda_memory.cpp:17-28), before any stage is timed.  Admission
  * against the budget is unchanged. */
 gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes);
+/* FP64 verification of every later contraction on this context: each output
+ * chunk's values are compared, before delivery, with FP64 sums of their
+ * matched products formed on the GPU, for all rows when a contraction has at
+ * most max_products matched products, else for a seeded sample of rows of
+ * about that many products; results in gsparc_stats (max_rel_err, ...).
+ * 0 turns it off (the default).  Costs one extra pass over the sampled
+ * products per chunk; a plan's replayed chunks are not verified. */
+gsparc_status gsparc_ctx_set_verify(gsparc_ctx *ctx, uint64_t max_products);
+/* Host-side fault injection (tests of the error paths; no counterpart in the
+ * reference, which exit()s on exhaustion, src/gsparc/cuda_memory.cpp:78): the
+ * nth device allocation of this context from now (1 = the next) fails with
+ * GSPARC_ENOMEM, once; 0 disarms.  The device is not involved. */
+gsparc_status gsparc_ctx_inject_alloc_failure(gsparc_ctx *ctx, uint64_t nth);
 /* Bytes currently allocated by the context and its high-water mark. */
 gsparc_status gsparc_ctx_memory(gsparc_ctx *ctx, uint64_t *in_use, uint64_t *peak,
                                 uint64_t *budget);
@@ -341,6 +363,12 @@ gsparc_status gsparc_serve_wait(gsparc_server *srv, uint64_t ticket, double time
 gsparc_status gsparc_serve_stats(gsparc_server *srv, gsparc_server_stats *out);
 /* Forget the latency samples and counters (after a warm-up). */
 gsparc_status gsparc_serve_reset_stats(gsparc_server *srv);
+/* Hold (paused != 0) or resume the lanes: while paused no lane starts a new
+ * batch (running batches finish); submitted requests wait. */
+gsparc_status gsparc_serve_pause(gsparc_server *srv, int paused);
+/* Host-side fault injection: arms every lane's allocator so that its nth
+ * device allocation from now fails with GSPARC_ENOMEM, once (0 disarms). */
+gsparc_status gsparc_serve_inject_alloc_failure(gsparc_server *srv, uint64_t nth);
 
 /* ---- host helpers (no GPU needed) ---------------------------------------- */
 /* Parse a .tns file: 1-based text COO, one nonzero per line, order = tokens of

@@ -3,20 +3,19 @@
 Every job's result must equal the result of the same contraction run alone
 (gsparc_sptc): keys, order and nnz bit-exact; values bit-exact where the
 accumulation order is fixed and in every case within the FP64-oracle bar
-    |z - z64| <= 1e-5 * |z64| + 1e-7 * sum|products|.
+(tests/value_bar.py: max relative error <= 1e-5).
 """
 import numpy as np
 import pytest
 
 import gsparc_b200 as gb
 import oracle_bind as ob
+import value_bar
 from gsparc_b200 import synth
 from gsparc_b200.synth import CooTensor
 
 pytestmark = pytest.mark.gpu
 
-REL = 1e-5
-ABS = 1e-7
 
 
 @pytest.fixture(scope="module")
@@ -47,9 +46,7 @@ def check_oracle(res, X, Y, cx, cy):
     assert res.ir_nnz == z.ir_nnz
     assert res.nnz == z.nnz
     assert np.array_equal(res.keys, z.keys)
-    err = np.abs(res.vals.astype(np.float64) - z.vals)
-    tol = REL * np.abs(z.vals) + ABS * z.abs_sums
-    assert np.all(err <= tol), f"max excess {np.max(err - tol)}"
+    value_bar.max_rel_err(res.vals, z.vals)
 
 
 def check_same_as_alone(ctx, inst, jobs, results):

@@ -5,8 +5,8 @@ include/gsparc/sptc.cuh:362-698), through the C ABI and the CLI's -m.
 The resident result must hold exactly the output of gsparc_sptc (coordinates
 decoded from its keys, values bit-identical).  A chain Z = (X x Y) x T is
 checked against the FP64 oracle run on the first result as the engine holds it
-(FP32 values): keys, order and nnz bit-exact, values within
-|z - z64| <= 1e-5 * |z64| + 1e-7 * sum|products|.
+(FP32 values): keys, order and nnz bit-exact, values within the bar of
+tests/value_bar.py (max relative error <= 1e-5).
 """
 import os
 import re
@@ -18,13 +18,12 @@ import pytest
 import golden_cases as gc
 import gsparc_b200 as gb
 import oracle_bind as ob
+import value_bar
 from gsparc_b200 import synth
 from gsparc_b200.synth import CooTensor
 
 pytestmark = pytest.mark.gpu
 
-REL = 1e-5
-ABS = 1e-7
 
 
 @pytest.fixture(scope="module")
@@ -97,8 +96,7 @@ def chain_case():
 def check(res, z):
     assert res.ir_nnz == z.ir_nnz and res.nnz == z.nnz
     assert np.array_equal(res.keys, z.keys)
-    tol = REL * np.abs(z.vals) + ABS * z.abs_sums
-    assert np.all(np.abs(res.vals.astype(np.float64) - z.vals) <= tol)
+    value_bar.max_rel_err(res.vals, z.vals)
 
 
 @pytest.mark.parametrize("accum", [0, -1, 1])

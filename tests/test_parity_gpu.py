@@ -1,9 +1,13 @@
 """Parity of the CUDA engine (through the C ABI) with the reference outputs and
 the FP64 oracle.
 
-Bars: output coordinates, order and nnz bit-exact; values within
-    |z - z64| <= 1e-5 * |z64| + 1e-7 * sum|products|
-of the FP64 oracle (the second term only matters for sums that cancel).
+Bars: output coordinates, order and nnz bit-exact; values: max relative error
+    |z - z64| / |z64| <= 1e-5
+against the FP64 oracle on every output whose FP64 value is nonzero, and
+exactly 0 where it is 0 (sums that cancel exactly).  The engine's compensated
+FP32 sums (TwoSum of every add plus each product's fma error) are within a few
+units in the last place of the exact sum, so this holds with cancelling N(0,1)
+sums too.
 """
 import numpy as np
 import pytest
@@ -17,7 +21,6 @@ from gsparc_b200.synth import CooTensor
 pytestmark = pytest.mark.gpu
 
 REL = 1e-5
-ABS = 1e-7
 
 
 @pytest.fixture(scope="module")
@@ -37,10 +40,11 @@ def check_vs_oracle(res, X, Y, cx, cy):
     assert res.nnz == z.nnz
     assert np.array_equal(res.keys, z.keys)
     err = np.abs(res.vals.astype(np.float64) - z.vals)
-    tol = REL * np.abs(z.vals) + ABS * z.abs_sums
-    assert np.all(err <= tol), f"max excess {np.max(err - tol)}"
-    nz = np.abs(z.vals) > 0
-    return float(np.max(err[nz] / np.abs(z.vals[nz]))) if nz.any() else 0.0
+    nz = z.vals != 0
+    assert np.all(err[~nz] == 0), "an exactly cancelling sum is not exactly 0"
+    rel = float(np.max(err[nz] / np.abs(z.vals[nz]))) if nz.any() else 0.0
+    assert rel <= REL, rel
+    return rel
 
 
 @pytest.mark.parametrize("accum", [0, -1, 1])
@@ -70,7 +74,7 @@ def test_workloads_reduced_scale(ctx, case, accum):
     X, Y, cx, cy = synth.WORKLOADS[case](scale=scale)
     res = run(ctx, X, Y, cx, cy, accum)
     rel = check_vs_oracle(res, X, Y, cx, cy)
-    assert rel <= REL or True  # bounded above by the tolerance check
+    print(f"{case} accum {accum}: max rel err vs FP64 {rel:.3e} over {res.nnz} outputs")
 
 
 def test_many_output_chunks_equal_one_chunk(ctx):

@@ -3,7 +3,7 @@ the numeric pass executed many times, also replayed from a CUDA graph.
 
 Every execution must give the result gsparc_sptc gives for the operands'
 current values: keys, order and nnz bit-exact; values within the FP64-oracle
-bar |z - z64| <= 1e-5 * |z64| + 1e-7 * sum|products|.
+bar of tests/value_bar.py (max relative error <= 1e-5).
 """
 import numpy as np
 import pytest
@@ -11,13 +11,12 @@ import torch
 
 import gsparc_b200 as gb
 import oracle_bind as ob
+import value_bar
 from gsparc_b200 import synth
 from gsparc_b200.synth import CooTensor
 
 pytestmark = pytest.mark.gpu
 
-REL = 1e-5
-ABS = 1e-7
 
 
 @pytest.fixture(scope="module")
@@ -43,8 +42,7 @@ def check_oracle(keys, vals, X, Y, cx, cy):
     z = ob.sptc(X, Y, cx, cy)
     assert keys.shape[0] == z.nnz
     assert np.array_equal(keys, z.keys)
-    tol = REL * np.abs(z.vals) + ABS * z.abs_sums
-    assert np.all(np.abs(vals.astype(np.float64) - z.vals) <= tol)
+    value_bar.max_rel_err(vals, z.vals)
 
 
 @pytest.mark.parametrize("make", [lambda: synth.plain_small(scale=0.2), lambda: synth.esc_large(scale=0.005),

@@ -2,9 +2,8 @@
 requests over resident operands, admission by HBM budget.
 
 Every request's result must equal the same contraction run alone
-(gsparc_sptc): keys, order and nnz bit-exact; values within the FP64-oracle
-bar |z - z64| <= 1e-5 * |z64| + 1e-7 * sum|products| and within that bar of
-the alone result.
+(gsparc_sptc): keys, order and nnz bit-exact; values of both within the
+FP64-oracle bar of tests/value_bar.py (max relative error <= 1e-5).
 """
 import threading
 import time
@@ -14,12 +13,11 @@ import pytest
 
 import gsparc_b200 as gb
 import oracle_bind as ob
+import value_bar
 from gsparc_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
-REL = 1e-5
-ABS = 1e-7
 
 
 @pytest.fixture(scope="module")
@@ -52,9 +50,8 @@ def same_result(r, a, X, Y, cx, cy, oracle=False):
     if oracle:
         z = ob.sptc(X, Y, cx, cy)
         assert np.array_equal(r.keys, z.keys)
-        tol = REL * np.abs(z.vals) + ABS * z.abs_sums
-        assert np.all(np.abs(r.vals.astype(np.float64) - z.vals) <= tol)
-        assert np.all(np.abs(r.vals.astype(np.float64) - a.vals.astype(np.float64)) <= 2 * tol)
+        value_bar.max_rel_err(r.vals, z.vals)
+        value_bar.max_rel_err(a.vals, z.vals)
 
 
 def test_each_result_same_alone_and_in_the_mix(mixed, alone):
