@@ -8,6 +8,6 @@ from .synth import CooTensor  # noqa: F401
 from .api import (  # noqa: F401
     ACCUM_AUTO, ACCUM_DENSE, ACCUM_ESC, Context, DeviceTensor, GsparcError, SpTC, SpTCResult,
     decode_keys, digest_chunk, splitmix64, index_match, layout, lib, linearize, plan_shards, read_tns, read_quantum, sort_pairs, sptc,
-    sptc_batch, Server, ServerTensor, sptc_resident, ResidentResult, autotune, Plan,
+    sptc_batch, sptc_host, Server, ServerTensor, sptc_resident, ResidentResult, autotune, Plan,
     version, write_tns, LIB_PATH, CLI_PATH, EXPORTS,
 )

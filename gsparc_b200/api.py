@@ -73,7 +73,8 @@ class Stats(ctypes.Structure):
                 ("heavy_windows", ctypes.c_uint64), ("stream_rows", ctypes.c_uint64),
                 ("verified_nnz", ctypes.c_uint64), ("verified_products", ctypes.c_uint64),
                 ("verify_mismatch", ctypes.c_uint64), ("verify_skipped_rows", ctypes.c_uint64),
-                ("max_rel_err", ctypes.c_double), ("max_abs_err", ctypes.c_double)]
+                ("max_rel_err", ctypes.c_double), ("max_abs_err", ctypes.c_double),
+                ("x_parts", ctypes.c_uint64), ("y_parts", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -83,7 +84,7 @@ _lib = None
 
 EXPORTS = [
     "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create", "gsparc_ctx_reserve",
-    "gsparc_ctx_set_verify", "gsparc_host_pin", "gsparc_host_unpin",
+    "gsparc_ctx_set_verify", "gsparc_ctx_set_tiles", "gsparc_host_pin", "gsparc_host_unpin",
     "gsparc_ctx_destroy", "gsparc_ctx_memory", "gsparc_tensor_upload", "gsparc_tensor_free",
     "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
     "gsparc_free_host", "gsparc_layout", "gsparc_plan_shards", "gsparc_linearize",
@@ -91,11 +92,15 @@ EXPORTS = [
     "gsparc_serve_create", "gsparc_serve_destroy", "gsparc_serve_upload", "gsparc_serve_release",
     "gsparc_serve_submit", "gsparc_serve_poll", "gsparc_serve_wait", "gsparc_serve_stats",
     "gsparc_serve_reset_stats", "gsparc_serve_pause", "gsparc_serve_inject_alloc_failure",
-    "gsparc_ctx_inject_alloc_failure", "gsparc_sptc_resident", "gsparc_tensor_download",
+    "gsparc_ctx_inject_alloc_failure", "gsparc_sptc_host", "gsparc_sptc_resident", "gsparc_tensor_download",
     "gsparc_read_quantum", "gsparc_autotune", "gsparc_plan_create", "gsparc_plan_chunks", "gsparc_plan_chunk",
     "gsparc_plan_job_output", "gsparc_plan_refresh", "gsparc_plan_execute", "gsparc_plan_check",
     "gsparc_plan_destroy", "gsparc_tensor_set_values",
 ]
+
+
+class _PartOpts(ctypes.Structure):
+    _fields_ = [("max_part_nnz_x", ctypes.c_uint64), ("max_part_nnz_y", ctypes.c_uint64)]
 
 
 class _Job(ctypes.Structure):
@@ -126,13 +131,17 @@ class ServeStats(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("accum", ctypes.c_int), ("max_chunk_nnz", ctypes.c_uint64), ("ms", ctypes.c_double),
                 ("cached", ctypes.c_int), ("ncandidates", ctypes.c_int), ("cand_accum", ctypes.c_int * 8),
-                ("cand_chunk", ctypes.c_uint64 * 8), ("cand_ms", ctypes.c_double * 8)]
+                ("cand_chunk", ctypes.c_uint64 * 8), ("cand_ms", ctypes.c_double * 8),
+                ("light_row_max", ctypes.c_uint64), ("heavy_window_cap", ctypes.c_uint32),
+                ("cand_light", ctypes.c_uint64 * 8), ("cand_cap", ctypes.c_uint32 * 8)]
 
     def as_dict(self) -> dict:
         n = self.ncandidates
         return {"accum": self.accum, "max_chunk_nnz": self.max_chunk_nnz, "ms": self.ms,
+                "light_row_max": self.light_row_max, "heavy_window_cap": self.heavy_window_cap,
                 "cached": bool(self.cached),
-                "candidates": [(self.cand_accum[i], self.cand_chunk[i], self.cand_ms[i]) for i in range(n)]}
+                "candidates": [(self.cand_accum[i], self.cand_chunk[i], self.cand_ms[i], self.cand_light[i],
+                                self.cand_cap[i]) for i in range(n)]}
 
 
 class Digest(ctypes.Structure):
@@ -160,6 +169,7 @@ def lib():
     L.gsparc_ctx_create.argtypes = [I, U64, ctypes.POINTER(P)]
     L.gsparc_ctx_reserve.argtypes = [P, U64]
     L.gsparc_ctx_set_verify.argtypes = [P, U64]
+    L.gsparc_ctx_set_tiles.argtypes = [P, U64, ctypes.c_uint32]
     L.gsparc_host_pin.argtypes = [P, U64]
     L.gsparc_host_unpin.argtypes = [P]
     L.gsparc_ctx_destroy.argtypes = [P]
@@ -171,6 +181,8 @@ def lib():
     L.gsparc_sptc.argtypes = [P, P, P, I, P, P, I, ctypes.POINTER(_Sink), ctypes.POINTER(Stats), P]
     L.gsparc_sptc_shard.argtypes = [P, P, P, I, P, P, I, I, I, ctypes.POINTER(_Sink),
                                     ctypes.POINTER(Stats), P]
+    L.gsparc_sptc_host.argtypes = [P, ctypes.POINTER(_Coo), ctypes.POINTER(_Coo), I, P, P, I,
+                                   ctypes.POINTER(_PartOpts), ctypes.POINTER(_Sink), ctypes.POINTER(Stats), P]
     L.gsparc_read_tns.argtypes = [ctypes.c_char_p, I, P, P, P, ctypes.POINTER(P), ctypes.POINTER(P)]
     L.gsparc_read_quantum.argtypes = [ctypes.c_char_p, I, P, P, P, ctypes.POINTER(P), ctypes.POINTER(P)]
     L.gsparc_write_tns.argtypes = [ctypes.c_char_p, I, U64, P, P]
@@ -308,6 +320,12 @@ class Context:
         """Host-side fault injection: the nth device allocation of this context
         from now (1 = the next) fails with GSPARC_ENOMEM, once; 0 disarms."""
         _check(lib().gsparc_ctx_inject_alloc_failure(self._h, nth), "ctx_inject_alloc_failure")
+
+    def set_tiles(self, light_row_max: int = 0, heavy_window_cap: int = 0):
+        """Accumulation tiles of later contractions (0 = defaults): rows of up to
+        light_row_max products use the on-chip ESC (<= 2048), heavy windows hold
+        at most heavy_window_cap outputs."""
+        _check(lib().gsparc_ctx_set_tiles(self._h, light_row_max, heavy_window_cap), "ctx_set_tiles")
 
     def set_verify(self, max_products: int):
         """FP64 verification of later contractions' outputs on the GPU (all rows
@@ -494,6 +512,68 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
     return SpTCResult(int(st.nnz), int(st.ir_nnz), keys, vals, st.as_dict())
 
 
+def _host_coo(t: CooTensor):
+    """A gsparc_coo over host arrays (and the arrays it points into)."""
+    dims = np.asarray([int(d) for d in t.dims], np.uint64)
+    idx = np.ascontiguousarray(t.idx, np.uint64)
+    val = np.ascontiguousarray(t.val, np.float32)
+    order = len(t.dims)
+    arr = (ctypes.c_void_p * max(order, 1))(*[idx[m].ctypes.data for m in range(order)])
+    coo = _Coo(order, dims.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), int(val.shape[0]), arr,
+               val.ctypes.data, 0)
+    return coo, (dims, idx, val, arr)
+
+
+def sptc_host(ctx: Context, X: CooTensor, Y: CooTensor, cx: Sequence[int], cy: Sequence[int],
+              dense_accumulator: int = ACCUM_AUTO, max_part_nnz_x: int = 0, max_part_nnz_y: int = 0,
+              sink: str = "host", max_chunk_nnz: int = 0, stream: int = 0, staging: int = 1 << 22) -> SpTCResult:
+    """Z = X x Y for host operands that need not fit the HBM budget
+    (gsparc_sptc_host): X is cut into output-row parts and Y into
+    output-column parts (of at most max_part_nnz_* nonzeros, or sized from the
+    budget), every pair is contracted, Z arrives in key order.  sink: "host"
+    (Z returned as numpy arrays) or "discard"."""
+    if len(cx) != len(cy):
+        raise ValueError("cx and cy must have the same length")
+    c1 = np.asarray(cx, np.int32)
+    c2 = np.asarray(cy, np.int32)
+    cox, kx = _host_coo(X)
+    coy, ky = _host_coo(Y)
+    opts = _PartOpts(max_part_nnz_x, max_part_nnz_y)
+    st = Stats()
+    s = _Sink()
+    s.max_chunk_nnz = max_chunk_nnz
+    keep = [kx, ky]
+    parts = []
+    if sink == "discard":
+        s.kind = SINK_DISCARD
+    elif sink == "host":
+        s.kind = SINK_HOST
+        hk = np.zeros(staging, np.uint64)
+        hv = np.zeros(staging, np.float32)
+
+        def _cb(user, k, v, n, first, on_dev):
+            kk = np.ctypeslib.as_array(ctypes.cast(k, ctypes.POINTER(ctypes.c_uint64)), shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+            vv = np.ctypeslib.as_array(ctypes.cast(v, ctypes.POINTER(ctypes.c_float)), shape=(n,)).copy() if n else np.zeros(0, np.float32)
+            parts.append((first, kk, vv))
+            return 0
+        s.host_keys = hk.ctypes.data
+        s.host_vals = hv.ctypes.data
+        s.host_capacity = staging
+        s.on_chunk = CHUNK_FN(_cb)
+        keep += [hk, hv, s.on_chunk]
+    else:
+        raise ValueError(f"unknown sink {sink!r}")
+    _check(lib().gsparc_sptc_host(ctx.handle, ctypes.byref(cox), ctypes.byref(coy), len(c1), _p(c1), _p(c2),
+                                  int(dense_accumulator), ctypes.byref(opts), ctypes.byref(s), ctypes.byref(st),
+                                  ctypes.c_void_p(stream)), "sptc_host")
+    keys = vals = None
+    if sink == "host":
+        parts.sort(key=lambda p: p[0])
+        keys = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0, np.uint64)
+        vals = np.concatenate([p[2] for p in parts]) if parts else np.zeros(0, np.float32)
+    return SpTCResult(int(st.nnz), int(st.ir_nnz), keys, vals, st.as_dict())
+
+
 class ResidentResult(DeviceTensor):
     """A contraction result kept on the device (gsparc_sptc_resident): a
     COO operand whose modes are X's free modes then Y's free modes."""
@@ -580,8 +660,10 @@ class Plan:
 
 def autotune(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: Sequence[int],
              retune: bool = False, stream: int = 0) -> dict:
-    """Measured choice of accumulator and output chunk size for Z = X x Y
-    (gsparc_autotune): {"accum", "max_chunk_nnz", "ms", "cached", "candidates"}."""
+    """Measured choice of accumulator, tiles and output chunk size for Z = X x Y
+    (gsparc_autotune): {"accum", "max_chunk_nnz", "light_row_max",
+    "heavy_window_cap", "ms", "cached", "candidates"}; candidates are
+    (accum, max_chunk_nnz, ms, light_row_max, heavy_window_cap)."""
     if len(cx) != len(cy):
         raise ValueError("cx and cy must have the same length")
     c1 = np.asarray(cx, np.int32)

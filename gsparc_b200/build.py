@@ -28,7 +28,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
               "-I" + os.path.join(ROOT, "include"), "-I" + CSRC] + ARCH
 LIB_SOURCES = ["util.cpp", "prep.cu", "accumulate.cu", "rowwin.cu", "engine.cu", "capi.cpp", "tns_io.cpp",
-               "noalloc.cu", "batch.cu", "stream.cu", "serve.cpp", "wide.cu", "chain.cu", "tune.cpp", "verify.cu"]
+               "noalloc.cu", "batch.cu", "stream.cu", "serve.cpp", "wide.cu", "chain.cu", "tune.cpp", "verify.cu",
+               "partition.cpp"]
 CLI_SOURCES = ["cli.cpp"]
 
 

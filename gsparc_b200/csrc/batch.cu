@@ -683,10 +683,16 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     const int g = (int)G.size();
     const int jb = ceil_log2((uint64_t)g);
     int kbx = 0, kby = 0;
+    uint64_t max_light = 0;
     for (Job *j : G) {
         kbx = std::max(kbx, j->LX.nbits());
         kby = std::max(kby, j->LY.nbits());
+        max_light = std::max(max_light, j->light_max);
     }
+    // light units hold rows whose first product falls in one bin of light_bin
+    // products: fewer than light_bin + light_max <= kLightCap products
+    const uint64_t light_bin = std::max<uint64_t>(
+        1, std::min<uint64_t>(kLightUnitMax - kLightRowMax, (uint64_t)kLightCap - std::min<uint64_t>(max_light, kLightCap - 1)));
     GS_REQUIRE(kbx + jb <= 64 && kby + jb <= 64, GSPARC_EINTERNAL, "batch group keys wider than 64 bits");
 
     cudaEvent_t *ev = ctx->ev;
@@ -885,7 +891,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
         select_idx(A, lnz, nx, L, cnts.get() + 4, s);
         if (nx) {
             k_bstart<<<grid_for(nx), kThreads, 0, s>>>(L, cnts.get() + 4, lpre, bc,
-                                                        (uint64_t)(kLightUnitMax - kLightRowMax), nx, heavy);
+                                                        light_bin, nx, heavy);
             count_launch();
             GS_CUDA(cudaGetLastError());
         }
@@ -954,6 +960,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     aa.row_off = row_off;
     aa.row_xi = row_xi;
     aa.err = ctx->d_flag;
+    aa.heavy_cap = ctx->heavy_window_cap;
     const int ghs = std::max(1, ctx->sm_count * heavy_blocks_per_sm(false));
     const int gh = std::max(1, ctx->sm_count * heavy_blocks_per_sm(true));
     const int gl = std::max(1, ctx->sm_count * light_blocks_per_sm());
@@ -1378,7 +1385,7 @@ void validate_jobs(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, cudaStream_t s,
                 q.LX = make_layout(2, q.tx->dims, 1, q.wide->cx2);
                 q.LY = make_layout(2, q.ty->dims, 1, q.wide->cy2);
             }
-            q.light_max = J.accum == GSPARC_ACCUM_DENSE ? 0 : kLightRowMax;
+            q.light_max = J.accum == GSPARC_ACCUM_DENSE ? 0 : (ctx->light_row_max ? ctx->light_row_max : kLightRowMax);
             q.width = std::max(q.LX.nbits(), q.LY.nbits());
             J.stats.nnz_x = J.x->nnz;
             J.stats.nnz_y = J.y->nnz;

@@ -129,6 +129,18 @@ gsparc_status gsparc_ctx_inject_alloc_failure(gsparc_ctx *ctx, uint64_t nth) {
     });
 }
 
+gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint32_t heavy_window_cap) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        GS_REQUIRE(light_row_max <= gs::kLightCap / 2, GSPARC_EINVAL,
+                   "light_row_max above " + std::to_string(gs::kLightCap / 2));
+        GS_REQUIRE(heavy_window_cap == 0 || (heavy_window_cap >= 256 && heavy_window_cap <= (uint32_t)gs::kHeavyCap),
+                   GSPARC_EINVAL, "heavy_window_cap must be 0 or 256.." + std::to_string(gs::kHeavyCap));
+        ctx->light_row_max = light_row_max;
+        ctx->heavy_window_cap = heavy_window_cap;
+    });
+}
+
 gsparc_status gsparc_ctx_set_verify(gsparc_ctx *ctx, uint64_t max_products) {
     return guard([&] {
         GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
@@ -286,6 +298,18 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
             st.stream_rows = bst.stream_rows;
             *stats = st;
         }
+    });
+}
+
+gsparc_status gsparc_sptc_host(gsparc_ctx *ctx, const gsparc_coo *X, const gsparc_coo *Y, int ncmodes,
+                               const int *cx, const int *cy, int accum, const gsparc_part_opts *opts,
+                               const gsparc_sink *sink, gsparc_stats *stats, void *stream) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        DeviceScope ds(ctx->device);
+        gsparc_sink discard{};
+        gs::sptc_partitioned(ctx, X, Y, ncmodes, cx, cy, accum, opts, sink ? sink : &discard, stats,
+                             (cudaStream_t)stream);
     });
 }
 

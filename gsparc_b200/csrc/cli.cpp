@@ -39,6 +39,7 @@ struct Opts {
     bool host_copy = false;  // -H
     bool verify = false;     // -V
     bool one_device = false; // -e: the -g row shards one after another on device 0
+    bool partition = false;  // -P: operands in parts from host memory (gsparc_sptc_host)
     int na = 0;
     std::vector<int> cz;
     bool tune = false;
@@ -52,12 +53,14 @@ struct Opts {
 void usage(const char *argv0) {
     std::fprintf(stderr,
                  "Usage: %s -X x.tns -Y y.tns -c N -x m1..mN -y m1..mN [-g G] [-n iters] [-d 1|0|-1] [-q]\n"
-                 "          [-m 1 -a K -z t1..tK] [-t] [-o z.tns | -H] [-V] [-e]\n"
+                 "          [-m 1 -a K -z t1..tK] [-t] [-o z.tns | -H] [-V] [-e] [-P]\n"
                  "  -H  copy every output chunk to page-locked host memory (and drop it there)\n"
                  "  -V  verify the values against FP64 sums on the GPU (all rows up to 2^28\n"
                  "      products, a seeded sample of rows above) and print the max errors\n"
                  "  -e  run the -g G row shards one after another on device 0 (their outputs\n"
-                 "      concatenate into the same Z as on G devices)\n",
+                 "      concatenate into the same Z as on G devices)\n"
+                 "  -P  contract from host memory in operand parts sized to the HBM budget (also\n"
+                 "      taken when the whole operands do not fit, with one GPU)\n",
                  argv0);
 }
 
@@ -217,7 +220,7 @@ int run_multi(const Opts &o, const Tensor &tx, const Tensor &ty) {
 int main(int argc, char **argv) {
     Opts o;
     int c;
-    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhvtHVe")) != -1) {
+    while ((c = getopt(argc, argv, "X:Y:c:a:m:x:y:z:n:g:d:o:qbhvtHVeP")) != -1) {
         switch (c) {
         case 'X':
             std::fprintf(stderr, "tensor X: %s\n", optarg);
@@ -288,6 +291,9 @@ int main(int argc, char **argv) {
             break;
         case 'e':
             o.one_device = true;
+            break;
+        case 'P':
+            o.partition = true;
             break;
         case 'b':
         case 'v':
@@ -373,6 +379,30 @@ int main(int argc, char **argv) {
             gsparc_coo cx{tx.order, tx.dims, tx.nnz, ix, tx.val, 0};
             gsparc_coo cy{ty.order, ty.dims, ty.nnz, iy, ty.val, 0};
             gsparc_tensor *X = nullptr, *Y = nullptr;
+            // operands in parts from host memory (FindPartitionNum / Partition,
+            // tensor_manager.tpp:33-61,634-886): asked for, or when they do not fit
+            auto run_parts = [&]() {
+                gsparc_sink sink{};
+                sink.kind = GSPARC_SINK_DISCARD;
+                std::vector<uint64_t> hk;
+                std::vector<float> hv;
+                if (!o.out.empty()) {
+                    sink.kind = GSPARC_SINK_HOST;
+                    hk.resize(1 << 24);
+                    hv.resize(1 << 24);
+                    sink.host_keys = hk.data();
+                    sink.host_vals = hv.data();
+                    sink.host_capacity = hk.size();
+                    sink.on_chunk = collect_chunk;
+                    sink.user = &parts[g];
+                }
+                return gsparc_sptc_host(ctx, &cx, &cy, o.nc, o.cx.data(), o.cy.data(), o.dense, nullptr, &sink,
+                                        &stats[g], nullptr);
+            };
+            if (o.partition) {
+                sts[g] = run_parts();
+                return;
+            }
             auto t0 = std::chrono::steady_clock::now();
             if (!(s = gsparc_tensor_upload(ctx, &cx, nullptr, &X)) &&
                 !(s = gsparc_tensor_upload(ctx, &cy, nullptr, &Y))) {
@@ -421,9 +451,13 @@ int main(int argc, char **argv) {
                     if (!s) {
                         accum = tn.accum;
                         sink.max_chunk_nnz = tn.max_chunk_nnz;
+                        s = gsparc_ctx_set_tiles(ctx, tn.light_row_max, tn.heavy_window_cap);
                         if (it == 0 && g == 0)
-                            std::fprintf(stderr, "autotune: dense_accumulator %d, chunk %llu, %.3f ms\n", tn.accum,
-                                         (unsigned long long)tn.max_chunk_nnz, tn.ms);
+                            std::fprintf(stderr,
+                                         "autotune: dense_accumulator %d, chunk %llu, light rows %llu, heavy window "
+                                         "%u, %.3f ms\n",
+                                         tn.accum, (unsigned long long)tn.max_chunk_nnz,
+                                         (unsigned long long)tn.light_row_max, tn.heavy_window_cap, tn.ms);
                     }
                 }
                 if (!s)
@@ -432,6 +466,12 @@ int main(int argc, char **argv) {
             }
             if (X) gsparc_tensor_free(ctx, X);
             if (Y) gsparc_tensor_free(ctx, Y);
+            if (s == GSPARC_ENOMEM && o.gpus == 1 && !o.host_copy) {
+                parts[g] = OutCollect{};
+                stats[g] = gsparc_stats{};
+                upload_ms[g] = 0;
+                s = run_parts();
+            }
             sts[g] = s;
         };
         std::vector<std::thread> th;

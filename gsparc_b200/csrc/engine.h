@@ -21,6 +21,12 @@ using JobDoneFn = std::function<void(gsparc_job *)>;
 void sptc_batch(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, uint64_t max_chunk_nnz, gsparc_stats *st,
                 cudaStream_t s, int shard = 0, int nshards = 1, const JobDoneFn *done_fn = nullptr);
 
+// Z = X x Y with operands in host memory, cut into parts that fit the budget
+// (partition.cpp).
+void sptc_partitioned(gsparc_ctx *ctx, const gsparc_coo *X, const gsparc_coo *Y, int nc, const int *cx,
+                      const int *cy, int accum, const gsparc_part_opts *opts, const gsparc_sink *sink,
+                      gsparc_stats *stats, cudaStream_t s);
+
 // Z = X x Y decoded into a resident COO tensor (chain.cu).
 void sptc_resident(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y, int nc, const int *cx,
                    const int *cy, int accum, gsparc_tensor **out, gsparc_stats *stats, cudaStream_t s);

@@ -143,6 +143,8 @@ struct gsparc_ctx {
     cudaStream_t copy_stream = nullptr;  // output chunk copies (non-blocking)
     cudaStream_t alt_stream = nullptr;   // every other output chunk's kernels (non-blocking)
     uint64_t verify_budget = 0;          // FP64 verification of outputs (0: off)
+    uint64_t light_row_max = 0;          // rows with at most this many products use the on-chip ESC (0: default)
+    uint32_t heavy_window_cap = 0;       // heavy rows: outputs per window (0: the compiled capacity)
 };
 
 struct gsparc_tensor {

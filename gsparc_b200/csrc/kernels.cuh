@@ -95,6 +95,7 @@ struct AccArgs {
     uint32_t *cursor;          // [nx] scratch (heavy path): next unprocessed Y entry per run
     uint32_t *pend;            // [nx] scratch (heavy path): end of the run's part in the window
     uint32_t ncols;            // distinct Y free indices (column ranks are < ncols)
+    uint32_t heavy_cap;        // heavy rows: outputs per window (0 or > kHeavyCap: kHeavyCap)
     // symbolic output
     uint32_t *row_nnz;         // [nrows]
     // numeric output

@@ -233,7 +233,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
     uint32_t *seg_off = seg_start + MAXR;                      // [MAXR + 4]
     uint32_t *seg_run = seg_off + MAXR + 4;                    // [MAXR]
     uint32_t *seg_cut = seg_run + MAXR;                        // [MAXR]
-    float *hi = reinterpret_cast<float *>(seg_cut + MAXR);     // [CAP]   (numeric)
+    float *seg_xv = reinterpret_cast<float *>(seg_cut + MAXR); // [MAXR]  (numeric) X value of each part
+    float *hi = seg_xv + (NUMERIC ? MAXR : 0);                 // [CAP]   (numeric)
     float *lo = hi + CAP;                                      // [CAP]   (numeric)
     uint32_t *ocol = wp;  // step 4 reuses the word prefix as the slot -> column table
     __shared__ uint32_t s_tmp[33];
@@ -242,6 +243,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
+    // outputs per window: the compiled capacity, or a smaller tile chosen at run time
+    const uint32_t cap = (a.heavy_cap && a.heavy_cap < (uint32_t)CAP) ? a.heavy_cap : (uint32_t)CAP;
 
     for (int i = tid; i < NWK; i += T) bits[i] = 0;
     if (NUMERIC)
@@ -273,7 +276,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         uint32_t rw = NUMERIC ? RW : RW_SYM;
         if (NUMERIC) {
             const uint64_t P = a.xprefix[xe] - a.xprefix[xs];
-            const uint64_t est = (uint64_t)CAP * ncols / (P ? P : 1);
+            const uint64_t est = (uint64_t)cap * ncols / (P ? P : 1);
             const uint64_t clamped = est < 32ull ? 32ull : (est > (uint64_t)RW ? (uint64_t)RW : est);
             rw = (uint32_t)clamped & ~31u;
         }
@@ -326,6 +329,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                 }
                 __syncthreads();
                 ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
+                if (NUMERIC)
+                    for (uint32_t k = tid; k < ns; k += T) seg_xv[k] = a.xval[seg_run[k]];
                 flat_for<RankItem>(
                     seg_start, seg_off, ns,
                     [&](uint32_t, uint32_t idx, RankItem &it) { it.r = a.yrank[idx]; },
@@ -367,18 +372,18 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             }
 
             // ---- numeric: cut the window at the CAP-th touched column if needed
-            const bool over = Dw > (uint32_t)CAP;
+            const bool over = Dw > cap;
             uint32_t R1 = lim, outputs = Dw;
             if (over) {
                 for (uint32_t w = w0; w < w1; ++w) {
-                    if (wp[w] <= (uint32_t)CAP && (uint32_t)CAP < wp[w] + __popc(bits[w])) {
-                        const uint32_t b = __fns(bits[w], 0u, (int)((uint32_t)CAP - wp[w] + 1));
+                    if (wp[w] <= cap && cap < wp[w] + __popc(bits[w])) {
+                        const uint32_t b = __fns(bits[w], 0u, (int)(cap - wp[w] + 1));
                         s_cut = R0 + 32u * w + b;
                     }
                 }
                 __syncthreads();
                 R1 = s_cut;
-                outputs = CAP;
+                outputs = cap;
             }
             __syncthreads();
 
@@ -397,13 +402,15 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                     }
                     __syncthreads();
                     ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
+                    for (uint32_t k = tid; k < ns; k += T) seg_xv[k] = a.xval[seg_run[k]];
+                    __syncthreads();
                 }
                 flat_for<ProdItem>(
                     seg_start, seg_off, ns,
                     [&](uint32_t k, uint32_t idx, ProdItem &it) {
                         it.r = a.yrank[idx];
                         it.yv = a.yval[idx];
-                        it.xv = a.xval[seg_run[k]];
+                        it.xv = seg_xv[k];
                     },
                     [&](uint32_t k, uint32_t idx, const ProdItem &it) {
                         if (it.r < R1) {
@@ -427,20 +434,22 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
 
             // ---- 4: slot -> column table, then coalesced writes of the window.
             // The word prefix is read into registers before the table overwrites it.
+            // Words go to threads cyclically (word tid + q*T), so a dense stretch of
+            // the bitmap spreads over many threads instead of a few.
             {
                 uint32_t myw[WPT_MAX], myp[WPT_MAX];
 #pragma unroll
                 for (int q = 0; q < WPT_MAX; ++q) {
-                    const uint32_t w = w0 + q;
-                    myw[q] = w < w1 ? bits[w] : 0u;
-                    myp[q] = w < w1 ? wp[w] : 0u;
+                    const uint32_t w = (uint32_t)tid + (uint32_t)q * T;
+                    myw[q] = w < nwu ? bits[w] : 0u;
+                    myp[q] = w < nwu ? wp[w] : 0u;
                 }
                 __syncthreads();
 #pragma unroll
                 for (int q = 0; q < WPT_MAX; ++q) {
                     uint32_t bw = myw[q];
                     uint32_t slot = myp[q];
-                    const uint32_t cbase = R0 + 32u * (w0 + q);
+                    const uint32_t cbase = R0 + 32u * ((uint32_t)tid + (uint32_t)q * T);
                     while (bw && slot < outputs) {
                         ocol[slot++] = cbase + (uint32_t)(__ffs(bw) - 1);
                         bw &= bw - 1;
@@ -472,7 +481,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                 __syncthreads();
                 R0 = R1;
             } else {
-                const uint64_t want = Dw ? (uint64_t)rw * (uint64_t)(15 * CAP / 16) / Dw : (uint64_t)rw * 4u;
+                const uint64_t want = Dw ? (uint64_t)rw * (uint64_t)(15 * cap / 16) / Dw : (uint64_t)rw * 4u;
                 uint64_t nr = want < (uint64_t)rw * 4u ? want : (uint64_t)rw * 4u;
                 nr = nr > (uint64_t)RW ? (uint64_t)RW : (nr < 32u ? 32u : nr);
                 rw = (uint32_t)nr & ~31u;
@@ -485,7 +494,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
 }
 
 size_t rowwin_smem(bool numeric) {
-    const size_t words = (numeric ? (size_t)NWORDS + WPN : (size_t)NWORDS_SYM) + MAXR + (MAXR + 4) + MAXR + MAXR;
+    const size_t words = (numeric ? (size_t)NWORDS + WPN + MAXR : (size_t)NWORDS_SYM) + MAXR + (MAXR + 4) + MAXR + MAXR;
     return words * 4 + (numeric ? (size_t)CAP * 8 : 0);
 }
 

@@ -119,6 +119,7 @@ typedef struct {
     uint64_t verify_skipped_rows; /* sampled rows past the FP64 scratch (unchecked) */
     double max_rel_err;         /* max |z - z64| / |z64| over checked z64 != 0   */
     double max_abs_err;         /* max |z - z64| over checked outputs            */
+    uint64_t x_parts, y_parts;  /* operand parts (gsparc_sptc_host; 0 otherwise) */
 } gsparc_stats;
 
 /* ---- version / errors ---------------------------------------------------- */
@@ -140,6 +141,14 @@ gsparc_status gsparc_ctx_destroy(gsparc_ctx *ctx);
  * (src/gsparc/cuda_memory.cpp:17-28), before any stage is timed.  Admission
  * against the budget is unchanged. */
 gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes);
+/* Tiles of the accumulation for later contractions on this context (0 = the
+ * defaults): rows with at most light_row_max matched products (<= 2048,
+ * default 1024) take the on-chip ESC, larger rows the windowed accumulator,
+ * whose windows hold at most heavy_window_cap outputs (256..7168, default
+ * 7168).  gsparc_autotune times candidates of both.  No counterpart in the
+ * reference, whose ESC and dense kernels have fixed launch shapes
+ * (include/gsparc/contraction.cuh:287-290,469-472). */
+gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint32_t heavy_window_cap);
 /* FP64 verification of every later contraction on this context: each output
  * chunk's values are compared, before delivery, with FP64 sums of their
  * matched products formed on the GPU, for all rows when a contraction has at
@@ -196,13 +205,15 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
  * reference, whose accumulator rule is fixed (include/gsparc/sptc.cuh:201-218).
  * gsparc_autotune runs the contraction (output discarded) with each candidate
  * -- accumulator ESC or DENSE (rows of up to 1024 products by the on-chip ESC,
- * or every row by the windowed dense accumulator), and output chunks of the
- * size the HBM budget allows, a quarter of it and a sixteenth -- times each
- * with CUDA events on `stream` and returns the fastest.  The choice is
- * remembered per operand shape (orders, dims, nnz, contract modes) for the
- * life of the process; a later call for the same shape returns it without
- * running anything unless `retune` is set.  Pass accum and max_chunk_nnz to
- * gsparc_sptc / a job's sink. */
+ * or every row by the windowed dense accumulator); then, for the better one,
+ * the tiles (light_row_max 256 or 2048 instead of 1024, a heavy window of half
+ * the outputs) and output chunks of the size the HBM budget allows, a quarter
+ * of it and a sixteenth -- times each with CUDA events on `stream` and returns
+ * the fastest.  The choice is remembered per operand shape (orders, dims,
+ * nnz, contract modes) for the life of the process; a later call for the same
+ * shape returns it without running anything unless `retune` is set.  Pass
+ * accum and max_chunk_nnz to gsparc_sptc / a job's sink and the tiles to
+ * gsparc_ctx_set_tiles.  The context's tiles are left as they were. */
 typedef struct {
     int accum;              /* GSPARC_ACCUM_ESC or GSPARC_ACCUM_DENSE        */
     uint64_t max_chunk_nnz; /* 0 = from the HBM budget                       */
@@ -212,6 +223,10 @@ typedef struct {
     int cand_accum[8];
     uint64_t cand_chunk[8];
     double cand_ms[8];
+    uint64_t light_row_max;     /* chosen tiles (gsparc_ctx_set_tiles)             */
+    uint32_t heavy_window_cap;
+    uint64_t cand_light[8];
+    uint32_t cand_cap[8];
 } gsparc_tuning;
 gsparc_status gsparc_autotune(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor *Y,
                               int ncmodes, const int *cx, const int *cy, int retune,
@@ -457,6 +472,26 @@ gsparc_status gsparc_index_match_noalloc(uint64_t nx, const uint64_t *d_xkeys, i
                                          uint64_t ny, const uint64_t *d_ykeys, int y_nfbits,
                                          uint64_t *d_pos, uint64_t *d_cnt, uint64_t *d_prefix,
                                          uint64_t *ir, void *stream);
+
+/* ---- operands larger than the HBM budget ---------------------------------- */
+/* Part sizes for gsparc_sptc_host (0 = derived from the context's budget). */
+typedef struct {
+    uint64_t max_part_nnz_x;  /* at most this many X nonzeros per X part       */
+    uint64_t max_part_nnz_y;  /* at most this many Y nonzeros per Y part       */
+} gsparc_part_opts;
+/* Z = X x Y for operands in HOST memory that need not fit the budget.  X is
+ * cut into parts at output-row ranges (X free index), Y into parts at
+ * output-column ranges (Y free index), each part gathered on the host and
+ * uploaded with the operand's dims; every (X part, Y part) pair is contracted
+ * and Z reaches the sink in key order (with several Y parts the outputs of
+ * one X part are merged on the host).  A single row or column is never split.
+ * Replaces FindPartitionNum / Partition / convert_and_sort and the part loop
+ * of SpTC (include/gsparc/tensor_manager.tpp:33-61,634-886,
+ * include/gsparc/sptc.cuh:42-139).  HOST sinks receive pieces in place while
+ * Z fits their arrays, in ring mode beyond; stats count the parts. */
+gsparc_status gsparc_sptc_host(gsparc_ctx *ctx, const gsparc_coo *X, const gsparc_coo *Y, int ncmodes,
+                               const int *cx, const int *cy, int accum, const gsparc_part_opts *opts,
+                               const gsparc_sink *sink, gsparc_stats *stats, void *stream);
 
 /* ---- verification digest of an output chunk ------------------------------ */
 /* Order-independent digest of n output nonzeros on the device: count, a sum

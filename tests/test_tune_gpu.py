@@ -1,8 +1,8 @@
 """The measured autotuner (gsparc_autotune) through the C ABI: it returns one of
 the candidates it timed, remembers its choice per operand shape, and a
-contraction run with the chosen settings gives the same result as the
-default (keys exact, values within |z - z64| <= 1e-5*|z64| + 1e-7*sum|products|
-of the FP64 oracle)."""
+contraction run with the chosen settings (accumulator, tiles, output chunk)
+gives the same result as the default (keys exact, values within the bar of
+tests/value_bar.py against the FP64 oracle)."""
 import subprocess
 
 import numpy as np
@@ -10,6 +10,7 @@ import pytest
 
 import gsparc_b200 as gb
 import oracle_bind as ob
+import value_bar
 from gsparc_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -31,18 +32,25 @@ def test_autotune_choice_and_result(ctx, make):
     try:
         t = gb.autotune(ctx, dx, dy, cx, cy, retune=True)
         assert not t["cached"] and len(t["candidates"]) >= 2
-        assert (t["accum"], t["max_chunk_nnz"], t["ms"]) in [tuple(c) for c in t["candidates"]]
+        choice = (t["accum"], t["max_chunk_nnz"], t["ms"], t["light_row_max"], t["heavy_window_cap"])
+        assert choice in [tuple(c) for c in t["candidates"]]
         assert t["ms"] == min(c[2] for c in t["candidates"])
         assert {c[0] for c in t["candidates"]} == {-1, 1}
+        # tile candidates: the heavy window at half its outputs, and for ESC the on-chip row limit
+        half = [c[4] for c in t["candidates"] if c[4]]
+        assert half, t["candidates"]
+        if t["accum"] == -1:
+            assert {256, 2048} <= {c[3] for c in t["candidates"]}
         again = gb.autotune(ctx, dx, dy, cx, cy)
         assert again["cached"] and again["accum"] == t["accum"] and again["max_chunk_nnz"] == t["max_chunk_nnz"]
-        tuned = gb.sptc(ctx, dx, dy, cx, cy, t["accum"], max_chunk_nnz=t["max_chunk_nnz"])
         base = gb.sptc(ctx, dx, dy, cx, cy)
-        assert np.array_equal(tuned.keys, base.keys)
         z = ob.sptc(X, Y, cx, cy)
-        assert np.array_equal(tuned.keys, z.keys)
-        tol = 1e-5 * np.abs(z.vals) + 1e-7 * z.abs_sums
-        assert np.all(np.abs(tuned.vals.astype(np.float64) - z.vals) <= tol)
+        for light, cap in {(t["light_row_max"], t["heavy_window_cap"]), (256, 0), (2048, 0), (0, half[0]), (0, 256)}:
+            ctx.set_tiles(light, cap)
+            tuned = gb.sptc(ctx, dx, dy, cx, cy, t["accum"], max_chunk_nnz=t["max_chunk_nnz"])
+            assert np.array_equal(tuned.keys, base.keys) and np.array_equal(tuned.keys, z.keys)
+            value_bar.max_rel_err(tuned.vals, z.vals)
+        ctx.set_tiles(0, 0)
     finally:
         dx.free()
         if dy is not dx:
