@@ -91,6 +91,10 @@ class Clocks:
         self.path = None
 
     def start(self):
+        """Starts sampling and returns once the first sample is written: the
+        sampler's start-up stalls the GPU for tens of milliseconds (measured:
+        34 ms on the first kernel after it starts), which must not fall into
+        the timed region."""
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -100,6 +104,13 @@ class Clocks:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 10 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
+        time.sleep(0.5)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -608,6 +619,10 @@ def ours_arm(args, world, rank, local, dist):
     torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()
+    flush.zero_()  # the first GPU work after the sampler starts absorbs its start-up stall
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     stats = []
