@@ -71,6 +71,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work per baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-stream (batched / served) lines")
     ap.add_argument("--mixed-count", type=int, default=256, help="instances of the batched / served streams")
+    ap.add_argument("--served-max-nnz", type=float, default=2e6,
+                    help="largest operand nnz of the served stream (the served workload's range reaches 5e7; "
+                         "the default keeps the default run within minutes)")
+    ap.add_argument("--served-only", action="store_true", help="run only the served stream (with its plain form)")
     ap.add_argument("--reference-gpu", action="store_true",
                     help="with --impl reference: time the reference GSPARC program itself on the GPU, and our "
                          "CLI on the same files, for the plain, ESC and dense-accumulator workloads")
@@ -377,14 +381,14 @@ def batched_stream(args, device, sp, stream):
 def served_stream(args, device, sp, stream):
     """The served workload, bounded so a run stays within minutes: 256 requests
     with operand orders 3-5, 1-2 contract modes, modes log-uniform 64..100k,
-    operand nnz from a power law n^-1.5 on [1e4, 2e6], Zipf s in [1.0,1.4]
+    operand nnz from a power law n^-1.5 on [1e4, --served-max-nnz (2e6)], Zipf s in [1.0,1.4]
     indices, U[-1,1) values, Poisson arrivals at a mean 2000/s (seed 5), into
     a gsparc_serve_* server with a 150 GB budget (less if the GPU has less
     free); the plain form answers the same arrivals one at a time."""
     import torch
     import gsparc_b200 as gb
     from gsparc_b200 import synth
-    inst, arrive = synth.served_stream(args.mixed_count, seed=5, max_nnz=2_000_000)
+    inst, arrive = synth.served_stream(args.mixed_count, seed=5, max_nnz=int(args.served_max_nnz))
     nnz = sum(X.nnz + Y.nnz for X, Y, _, _ in inst)
     free_b, _ = torch.cuda.mem_get_info()
     budget = min(150 << 30, int(free_b * 0.8))
@@ -441,7 +445,8 @@ def served_stream(args, device, sp, stream):
     wide = sum(1 for X, Y, _, _ in inst
                if sum(synth._bits(d) for d in X.dims) > 64 or sum(synth._bits(d) for d in Y.dims) > 64)
     desc = (f"{len(inst)} requests, {nnz} operand nonzeros, {ir:.4e} matched products (operand orders 3-5, "
-            "1-2 contract modes, modes log-uniform 64..100k, nnz power law n^-1.5 on [1e4, 2e6], Zipf s 1.0-1.4, "
+            f"1-2 contract modes, modes log-uniform 64..100k, nnz power law n^-1.5 on [1e4, {args.served_max_nnz:.0e}], "
+            "Zipf s 1.0-1.4, "
             f"U[-1,1), {wide} with operand keys over 64 bits, seed 5); Poisson arrivals, mean 2000/s; "
             f"HBM budget {budget / 2**30:.0f} GiB")
     return {"workload": desc, "unit": UNIT, "value": sst["products_per_s"], "p50_ms": sst["p50_ms"],
@@ -595,6 +600,11 @@ def ours_arm(args, world, rank, local, dist):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.served_only:
+        stream = torch.cuda.current_stream(dev)
+        if rank == 0:
+            print(json.dumps({"served": served_stream(args, local, stream.cuda_stream, stream)}), flush=True)
+        return
     # one contraction; with N ranks each contracts its row shard (rows of about
     # equal matched-product mass, the reference's per-GPU partition loop)
     X, _, cx, cy = workload(0, args.scale)

@@ -56,7 +56,8 @@ CHUNK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctyp
 class _Sink(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("on_chunk", CHUNK_FN), ("user", ctypes.c_void_p),
                 ("host_keys", ctypes.c_void_p), ("host_vals", ctypes.c_void_p),
-                ("host_capacity", ctypes.c_uint64), ("max_chunk_nnz", ctypes.c_uint64)]
+                ("host_capacity", ctypes.c_uint64), ("max_chunk_nnz", ctypes.c_uint64),
+                ("key_words", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -434,14 +435,17 @@ class SpTCResult:
 def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: Sequence[int],
          dense_accumulator: int = ACCUM_AUTO, sink: str = "host", max_chunk_nnz: int = 0,
          shard: int = 0, nshards: int = 1, stream: int = 0, on_chunk=None,
-         host_keys: Optional[np.ndarray] = None, host_vals: Optional[np.ndarray] = None) -> SpTCResult:
+         host_keys: Optional[np.ndarray] = None, host_vals: Optional[np.ndarray] = None,
+         key_words: int = 1) -> SpTCResult:
     """Z = X x_{cx,cy} Y on resident operands.
 
     sink: "host" (Z copied into numpy arrays), "discard" (computed chunk-wise
     in HBM and dropped, like the reference), "device" (``on_chunk(keys_ptr,
     vals_ptr, n, first)`` gets device pointers per chunk) or "ring" (chunks
     stream through the given ``host_keys``/``host_vals`` arrays, ``on_chunk``
-    sees numpy views).
+    sees numpy views).  key_words=2 delivers 128-bit keys (needed when X's
+    and Y's free bits exceed 64 together): with the host sink, keys come back
+    as an (n, 2) uint64 array, low word first.
     """
     if len(cx) != len(cy):
         raise ValueError("cx and cy must have the same length")
@@ -450,6 +454,8 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
     st = Stats()
     s = _Sink()
     s.max_chunk_nnz = max_chunk_nnz
+    s.key_words = key_words
+    kw = 2 if key_words == 2 else 1
     keep = []
     keys = vals = None
     if sink == "discard":
@@ -470,18 +476,18 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
             parts = []
 
             def _cbh(user, k, v, n, first, on_dev):
-                if first and k == s.host_keys + 8 * first:
+                if first and k == s.host_keys + 8 * kw * first:
                     return 0  # whole-Z mode: the chunk already sits at its final place
-                kk = np.ctypeslib.as_array(ctypes.cast(k, ctypes.POINTER(ctypes.c_uint64)), shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+                kk = np.ctypeslib.as_array(ctypes.cast(k, ctypes.POINTER(ctypes.c_uint64)), shape=(kw * n,)).copy() if n else np.zeros(0, np.uint64)
                 vv = np.ctypeslib.as_array(ctypes.cast(v, ctypes.POINTER(ctypes.c_float)), shape=(n,)).copy() if n else np.zeros(0, np.float32)
                 parts.append((first, kk, vv))
                 return 0
             cap = 1 << 22
-            hk = np.zeros(cap, np.uint64) if host_keys is None else host_keys
+            hk = np.zeros(kw * cap, np.uint64) if host_keys is None else host_keys
             hv = np.zeros(cap, np.float32) if host_vals is None else host_vals
             s.host_keys = hk.ctypes.data
             s.host_vals = hv.ctypes.data
-            s.host_capacity = min(hk.shape[0], hv.shape[0])
+            s.host_capacity = min(hk.shape[0] // kw, hv.shape[0])
             s.on_chunk = CHUNK_FN(_cbh)
             keep += [s.on_chunk, hk, hv]
         else:
@@ -489,10 +495,10 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
                 raise ValueError("ring sink needs host_keys and host_vals")
             s.host_keys = host_keys.ctypes.data
             s.host_vals = host_vals.ctypes.data
-            s.host_capacity = min(host_keys.shape[0], host_vals.shape[0])
+            s.host_capacity = min(host_keys.shape[0] // kw, host_vals.shape[0])
             if on_chunk is not None:
                 def _cbr(user, k, v, n, first, on_dev):
-                    return int(bool(on_chunk(host_keys[:n], host_vals[:n], n, first)))
+                    return int(bool(on_chunk(host_keys[: kw * n], host_vals[:n], n, first)))
                 s.on_chunk = CHUNK_FN(_cbr)
                 keep.append(s.on_chunk)
     else:
@@ -504,11 +510,13 @@ def sptc(ctx: Context, X: DeviceTensor, Y: DeviceTensor, cx: Sequence[int], cy: 
         parts.sort(key=lambda p: p[0])
         if st.nnz <= s.host_capacity:
             # whole Z fits the staging arrays: chunks landed in order
-            keys = np.array(np.ctypeslib.as_array(ctypes.cast(s.host_keys, ctypes.POINTER(ctypes.c_uint64)), shape=(s.host_capacity,))[: st.nnz])
+            keys = np.array(np.ctypeslib.as_array(ctypes.cast(s.host_keys, ctypes.POINTER(ctypes.c_uint64)), shape=(kw * s.host_capacity,))[: kw * st.nnz])
             vals = np.array(np.ctypeslib.as_array(ctypes.cast(s.host_vals, ctypes.POINTER(ctypes.c_float)), shape=(s.host_capacity,))[: st.nnz])
         else:
             keys = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0, np.uint64)
             vals = np.concatenate([p[2] for p in parts]) if parts else np.zeros(0, np.float32)
+        if kw == 2:
+            keys = keys.reshape(-1, 2)
     return SpTCResult(int(st.nnz), int(st.ir_nnz), keys, vals, st.as_dict())
 
 
@@ -1006,12 +1014,24 @@ def splitmix64(k: np.ndarray) -> np.ndarray:
 
 
 def decode_keys(keys: np.ndarray, x_dims, y_dims, cx, cy) -> np.ndarray:
-    """Output keys -> coordinates [X free modes ascending, Y free modes ascending]."""
+    """Output keys -> coordinates [X free modes ascending, Y free modes ascending].
+    keys: uint64 keys, or (n, 2) uint64 128-bit keys (low word first)."""
     bx, sx, icx, ncx, nfx = layout(x_dims, cx)
     by, sy, icy, ncy, nfy = layout(y_dims, cy)
     k = np.asarray(keys, np.uint64)
-    xf = k >> np.uint64(nfy) if nfy < 64 else np.zeros_like(k)
-    yf = k & np.uint64((1 << nfy) - 1) if nfy < 64 else k
+    if k.ndim == 2:  # 128-bit keys: x_f << nfy | y_f with x_f, y_f of at most 64 bits each
+        lo, hi = k[:, 0], k[:, 1]
+        if nfy == 0:
+            xf, yf = lo, np.zeros_like(lo)
+        elif nfy >= 64:
+            xf, yf = hi, lo
+        else:
+            xf = (hi << np.uint64(64 - nfy)) | (lo >> np.uint64(nfy))
+            yf = lo & np.uint64((1 << nfy) - 1)
+        k = lo
+    else:
+        xf = k >> np.uint64(nfy) if nfy < 64 else np.zeros_like(k)
+        yf = k & np.uint64((1 << nfy) - 1) if nfy < 64 else k
     cols = []
     for m in range(len(x_dims)):
         if not icx[m]:

@@ -603,6 +603,7 @@ struct Job {
     Layout LX, LY;
     uint64_t light_max;
     int width;          // widest operand key
+    int key_words = 1;  // output key words delivered to the sink (2: 128-bit keys)
     bool done = false;  // reported through the completion callback
 };
 
@@ -642,32 +643,34 @@ struct GroupPlan {
     const uint32_t *heavy_list() const { return Hc.get() ? Hc.get() : (H2.get() ? H2.get() : H.get()); }
 };
 
-// Delivers [dk, dk + n) of a job's output (first = offset inside the job).
+// Delivers [dk, dk + n) of a job's output (first = offset inside the job);
+// kw = key words per nonzero (2: 128-bit keys, dk holds 2n words).
 void deliver_slice(gsparc_sink &sink, const uint64_t *dk, const float *dv, uint64_t n, uint64_t first,
-                   uint64_t job_nnz, cudaStream_t s2, gsparc_stats &st, uint64_t &bytes_d2h) {
+                   uint64_t job_nnz, cudaStream_t s2, gsparc_stats &st, uint64_t &bytes_d2h, int kw = 1) {
     if (n == 0) return;
     if (sink.kind == GSPARC_SINK_DEVICE) {
         const uint64_t step = sink.max_chunk_nnz ? sink.max_chunk_nnz : n;
         for (uint64_t off = 0; off < n; off += step) {
             const uint64_t m = std::min(step, n - off);
-            if (sink.on_chunk(sink.user, dk + off, dv + off, m, first + off, 1))
+            if (sink.on_chunk(sink.user, dk + kw * off, dv + off, m, first + off, 1))
                 fail(GSPARC_ECALLBACK, "output callback stopped the contraction");
         }
         ++st.chunks;
     } else if (sink.kind == GSPARC_SINK_HOST) {
         if (sink.host_capacity >= job_nnz) {
-            d2h(sink.host_keys + first, dk, n, s2);
+            d2h(sink.host_keys + kw * first, dk, kw * n, s2);
             d2h(sink.host_vals + first, dv, n, s2);
-            bytes_d2h += 12 * n;
+            bytes_d2h += (8 * kw + 4) * n;
             GS_CUDA(cudaStreamSynchronize(s2));
-            if (sink.on_chunk && sink.on_chunk(sink.user, sink.host_keys + first, sink.host_vals + first, n, first, 0))
+            if (sink.on_chunk &&
+                sink.on_chunk(sink.user, sink.host_keys + kw * first, sink.host_vals + first, n, first, 0))
                 fail(GSPARC_ECALLBACK, "output callback stopped the contraction");
         } else {
             for (uint64_t off = 0; off < n; off += sink.host_capacity) {
                 const uint64_t m = std::min<uint64_t>(sink.host_capacity, n - off);
-                d2h(sink.host_keys, dk + off, m, s2);
+                d2h(sink.host_keys, dk + kw * off, kw * m, s2);
                 d2h(sink.host_vals, dv + off, m, s2);
-                bytes_d2h += 12 * m;
+                bytes_d2h += (8 * kw + 4) * m;
                 GS_CUDA(cudaStreamSynchronize(s2));
                 if (sink.on_chunk && sink.on_chunk(sink.user, sink.host_keys, sink.host_vals, m, first + off, 0))
                     fail(GSPARC_ECALLBACK, "output callback stopped the contraction");
@@ -1164,9 +1167,13 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     for (auto &c : chunks) bufn = std::max(bufn, c.n);
     DBuf<uint64_t> out_k[2];
     DBuf<float> out_v[2];
+    DBuf<uint64_t> out_k2[2];  // 128-bit keys of jobs whose sink asks for two key words
+    bool any_kw2 = false;
+    for (Job *q : G) any_kw2 |= q->key_words == 2;
     for (int i = 0; i < nbuf; ++i) {
         out_k[i].reset(A, std::max<uint64_t>(bufn, 1), s);
         out_v[i].reset(A, std::max<uint64_t>(bufn, 1), s);
+        if (any_kw2) out_k2[i].reset(A, 2 * std::max<uint64_t>(bufn, 1), s);
     }
     std::vector<cudaEvent_t> kev(2 * chunks.size(), nullptr);
     for (auto &e : kev) GS_CUDA(cudaEventCreate(&e));
@@ -1259,6 +1266,15 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
             gsparc_job &J = *G[j]->job;
             const uint64_t a0 = std::max(c0, job_first[j]), a1 = std::min(c1, job_first[j + 1]);
             if (a1 <= a0 || J.status != GSPARC_OK) continue;
+            if (G[j]->wide && G[j]->key_words == 2) {
+                // relabeled output keys back to x_f << Y_nfbits | y_f in 128 bits
+                uint64_t *k2 = out_k2[bi].get() + 2 * (a0 - c0);
+                wide_remap_keys128(*G[j]->wide, out_k[bi].get() + (a0 - c0), k2, a1 - a0, s2);
+                GS_CUDA(cudaStreamSynchronize(s2));
+                deliver_slice(J.sink, k2, out_v[bi].get() + (a0 - c0), a1 - a0, a0 - job_first[j], job_nnz[j],
+                              s2, J.stats, bst.bytes_d2h, 2);
+                continue;
+            }
             if (G[j]->wide) {
                 // relabeled output keys back to x_f << Y_nfbits | y_f
                 wide_remap_keys(*G[j]->wide, out_k[bi].get() + (a0 - c0), a1 - a0, s2);
@@ -1372,13 +1388,19 @@ void validate_jobs(gsparc_ctx *ctx, gsparc_job *jobs, int njobs, cudaStream_t s,
             for (int m = 0; m < J.ncmodes; ++m)
                 GS_REQUIRE(q.LX.bits[J.cx[m]] == q.LY.bits[J.cy[m]], GSPARC_EINVAL,
                            "contract modes of X and Y have different bit widths (mode sizes differ)");
-            GS_REQUIRE(q.LX.nfbits + q.LY.nfbits <= 64, GSPARC_EUNSUPPORTED,
-                       "output key wider than 64 bits (X free bits + Y free bits > 64)");
+            // a discarded output of more than 64 bits needs no key words at all:
+            // run it on the 128-bit path and deliver nothing
+            q.key_words = k.key_words ? k.key_words
+                                      : (k.kind == GSPARC_SINK_DISCARD && q.LX.nfbits + q.LY.nfbits > 64 ? 2 : 1);
+            GS_REQUIRE(q.key_words == 1 || q.key_words == 2, GSPARC_EINVAL, "sink key_words must be 0, 1 or 2");
+            GS_REQUIRE(q.LX.nfbits + q.LY.nfbits <= 64 * q.key_words, GSPARC_EUNSUPPORTED,
+                       "output key wider than 64 bits (X free bits + Y free bits > 64): set sink.key_words = 2");
             GS_REQUIRE(J.x->nnz < kMaxGroupNnz && J.y->nnz < kMaxGroupNnz, GSPARC_EUNSUPPORTED,
                        "operand with more than 2^31 nonzeros");
             const Layout LX0 = q.LX, LY0 = q.LY;
-            if (q.LX.nbits() > 64 || q.LY.nbits() > 64) {
-                // the reference's 128-bit key path: relabel onto 64-bit keys
+            if (q.LX.nbits() > 64 || q.LY.nbits() > 64 || q.key_words == 2) {
+                // the reference's 128-bit key path: relabel onto 64-bit keys (128-bit
+                // output keys are built from the rank tables at delivery)
                 q.wide = make_wide(ctx->arena, J.x, q.LX, J.y, q.LY, s);
                 q.tx = &q.wide->x2;
                 q.ty = &q.wide->y2;

@@ -73,18 +73,19 @@ struct Tensor {
 };
 
 struct OutCollect {
-    std::vector<uint64_t> keys;
+    std::vector<uint64_t> keys;  // kw words per nonzero (2: 128-bit keys, low word first)
     std::vector<float> vals;
+    int kw = 1;
 };
 
 int collect_chunk(void *user, const uint64_t *k, const float *v, uint64_t n, uint64_t first, int on_device) {
     (void)on_device;
     auto *c = static_cast<OutCollect *>(user);
-    if (c->keys.size() < first + n) {
-        c->keys.resize(first + n);
+    if (c->vals.size() < first + n) {
+        c->keys.resize(c->kw * (first + n));
         c->vals.resize(first + n);
     }
-    std::memcpy(c->keys.data() + first, k, 8 * n);
+    std::memcpy(c->keys.data() + c->kw * first, k, 8 * c->kw * n);
     std::memcpy(c->vals.data() + first, v, 4 * n);
     return 0;
 }
@@ -117,6 +118,14 @@ void print_report(double slitom, double idxmatch, double contraction, double dpr
     std::fprintf(stderr, "\n\n");
 }
 
+// Key words of the output: 2 when X's free bits + Y's free bits exceed 64.
+int out_words(const Tensor &tx, const std::vector<int> &cx, const Tensor &ty, const std::vector<int> &cy, int nc) {
+    int b[32], sh[32], ic[32], ncb, nfx, nfy;
+    gsparc_layout(tx.order, tx.dims, nc, cx.data(), b, sh, ic, &ncb, &nfx);
+    gsparc_layout(ty.order, ty.dims, nc, cy.data(), b, sh, ic, &ncb, &nfy);
+    return nfx + nfy > 64 ? 2 : 1;
+}
+
 // Output keys -> coordinates (X free modes ascending, then Y free modes), written as .tns.
 void write_output(const std::string &path, const OutCollect &out, int xo, const uint64_t *xd, const int *cx,
                   int yo, const uint64_t *yd, const int *cy, int nc) {
@@ -127,12 +136,14 @@ void write_output(const std::string &path, const OutCollect &out, int xo, const 
     for (int m = 0; m < xo; ++m) if (!icx[m]) fmx.push_back(m);
     for (int m = 0; m < yo; ++m) if (!icy[m]) fmy.push_back(m);
     const int zo = (int)(fmx.size() + fmy.size());
-    const uint64_t zn = out.keys.size();
+    const uint64_t zn = out.vals.size();
     std::vector<uint64_t> zi((size_t)zo * zn);
     for (uint64_t k = 0; k < zn; ++k) {
-        uint64_t key = out.keys[k];
-        uint64_t xf = nfy >= 64 ? 0 : key >> nfy;
-        uint64_t yf = nfy >= 64 ? key : key & ((1ull << nfy) - 1);
+        // the key is x_f << nfy | y_f, in one word or (kw == 2) in two
+        const unsigned __int128 key = out.kw == 2 ? ((unsigned __int128)out.keys[2 * k + 1] << 64) | out.keys[2 * k]
+                                                  : (unsigned __int128)out.keys[k];
+        uint64_t xf = (uint64_t)(key >> nfy);
+        uint64_t yf = nfy >= 64 ? (uint64_t)key : (uint64_t)key & ((1ull << nfy) - 1);
         int z = 0;
         for (int m : fmx) zi[(size_t)(z++) * zn + k] = (xf >> shx[m]) & ((bx[m] >= 64) ? ~0ull : ((1ull << bx[m]) - 1));
         for (int m : fmy) zi[(size_t)(z++) * zn + k] = (yf >> shy[m]) & ((by[m] >= 64) ? ~0ull : ((1ull << by[m]) - 1));
@@ -434,12 +445,16 @@ int main(int argc, char **argv) {
                     return;
                 }
                 if (!o.out.empty()) {
+                    // output keys over 64 bits come as two words each
+                    const int kw = out_words(tx, o.cx, ty, o.cy, o.nc);
+                    parts[g].kw = kw;
                     sink.kind = GSPARC_SINK_HOST;
-                    hk.resize(1 << 24);
+                    sink.key_words = kw;
+                    hk.resize((size_t)kw << 24);
                     hv.resize(1 << 24);
                     sink.host_keys = hk.data();
                     sink.host_vals = hv.data();
-                    sink.host_capacity = hk.size();
+                    sink.host_capacity = hv.size();
                     sink.on_chunk = collect_chunk;
                     sink.user = &parts[g];
                 }
@@ -505,6 +520,7 @@ int main(int argc, char **argv) {
         if (it == 0 && !o.out.empty()) {
             uint64_t base = 0;
             for (int g = 0; g < o.gpus; ++g) {
+                out.kw = parts[g].kw;
                 out.keys.insert(out.keys.end(), parts[g].keys.begin(), parts[g].keys.end());
                 out.vals.insert(out.vals.end(), parts[g].vals.begin(), parts[g].vals.end());
                 base += parts[g].keys.size();

@@ -16,7 +16,10 @@
 // hold, and runs them as one gsparc_sptc_batch.  Requests arriving meanwhile
 // queue up for the next free lane, so the batches of different lanes overlap
 // on the device: one lane's host-side planning and output delivery run while
-// another lane's kernels occupy the GPU.  A request whose output exceeds the
+// another lane's kernels occupy the GPU.  A large batch (2^21 operand
+// nonzeros or more) fills the GPU by itself and runs alone: overlapping it
+// with others only made both slower (measured on the served workload).  A
+// request whose output exceeds the
 // memory it was admitted with streams its output in chunks (the engine's
 // memory-aware partitioning), so admission only has to cover the operands'
 // working set and a bounded output window.
@@ -68,6 +71,9 @@ uint64_t job_estimate(const gsparc_job &J) {
 // half of what the batch leaves free.  The window only bounds the chunk size:
 // chunk buffers are allocated for the output that exists, so a generous
 // window costs nothing for small outputs and keeps large ones in few chunks.
+// Batches with at least this many operand nonzeros (X + Y) run alone.
+constexpr uint64_t kExclusiveNnz = 1ull << 21;
+
 uint64_t output_window(uint64_t max_ny, uint64_t free_after) {
     const uint64_t w = std::max<uint64_t>(128ull << 20, 64ull * max_ny + (16ull << 20));
     return std::max(w, free_after / 2);
@@ -94,6 +100,7 @@ struct gsparc_server {
     int running = 0;
     bool stop = false;
     bool paused = false;  // gsparc_serve_pause: lanes take no new batch
+    bool exclusive_running = false;  // a large batch runs alone
 
     // statistics
     std::vector<double> lat_ms;
@@ -258,11 +265,21 @@ void lane_main(gsparc_server *S, Lane *L) {
             S->cv_work.wait(lk);  // a completion frees memory
             continue;
         }
+        // Lane concurrency adapts to size: a large batch (at least
+        // kExclusiveNnz operand nonzeros) fills the GPU by itself, so it runs
+        // alone -- it waits for the running batches to finish and no other
+        // batch starts beside it.  Small batches overlap freely.
+        const bool exclusive = nz >= kExclusiveNnz;
+        if (S->exclusive_running || (exclusive && S->running > 0)) {
+            S->cv_work.wait(lk);
+            continue;
+        }
         for (Req *r : batch) r->taken = true;
         S->queue.erase(std::remove_if(S->queue.begin(), S->queue.end(), [](const Req *r) { return r->taken; }),
                        S->queue.end());
         S->reserved += reserve;
         S->running += 1;
+        S->exclusive_running = exclusive;
         S->peak_reserved = std::max(S->peak_reserved, S->reserved);
         S->max_in_flight = std::max<uint64_t>(S->max_in_flight, S->running);
         S->batches += 1;
@@ -274,6 +291,7 @@ void lane_main(gsparc_server *S, Lane *L) {
         lk.lock();
         S->reserved -= reserve;
         S->running -= 1;
+        if (exclusive) S->exclusive_running = false;
         S->cv_done.notify_all();
         S->cv_work.notify_all();
     }

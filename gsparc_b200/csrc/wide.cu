@@ -125,6 +125,31 @@ __global__ void k_wide_remap(uint64_t *__restrict__ keys, uint64_t n, const uint
     }
 }
 
+// (x_f << nfbits_y) | y_f as 128 bits: x_f and y_f each fit 64 bits
+__global__ void k_wide_remap128(const uint64_t *__restrict__ keys, uint64_t *__restrict__ out2, uint64_t n,
+                                const uint64_t *__restrict__ xf, const uint64_t *__restrict__ yf, int yb2,
+                                int nfbits_y) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t ymask = (1ull << yb2) - 1;  // yb2 <= 31
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = keys[i];
+        const uint64_t x = xf[k >> yb2], y = yf[k & ymask];
+        uint64_t lo, hi;
+        if (nfbits_y == 0) {
+            lo = x;
+            hi = 0;
+        } else if (nfbits_y >= 64) {
+            lo = y;
+            hi = x;
+        } else {
+            lo = (x << nfbits_y) | y;
+            hi = x >> (64 - nfbits_y);
+        }
+        out2[2 * i] = lo;
+        out2[2 * i + 1] = hi;
+    }
+}
+
 template <class T>
 void sort_pairs_u32(Arena &A, uint64_t n, const T *k_in, T *k_out, const uint32_t *v_in, uint32_t *v_out,
                     int bits, cudaStream_t s) {
@@ -264,6 +289,13 @@ std::unique_ptr<WideMap> make_wide(Arena &A, const gsparc_tensor *X, const Layou
     w->y2.owned = false;
     w->yb2 = mode_bits(w->y2.dims[1]);
     return w;
+}
+
+void wide_remap_keys128(const WideMap &w, const uint64_t *keys, uint64_t *out2, uint64_t n, cudaStream_t s) {
+    if (n == 0) return;
+    k_wide_remap128<<<grid_of(n), kT, 0, s>>>(keys, out2, n, w.xf, w.yf, w.yb2, w.nfbits_y);
+    count_launch();
+    GS_CUDA(cudaGetLastError());
 }
 
 void wide_remap_keys(const WideMap &w, uint64_t *keys, uint64_t n, cudaStream_t s) {

@@ -22,5 +22,7 @@ std::unique_ptr<WideMap> make_wide(Arena &A, const gsparc_tensor *X, const Layou
                                    const Layout &LY, cudaStream_t s);
 // Output keys of X' x Y' -> output keys of X x Y, in place, on stream s.
 void wide_remap_keys(const WideMap &w, uint64_t *keys, uint64_t n, cudaStream_t s);
+// The same as 128-bit keys, two words per key (low word first) into out2[2n].
+void wide_remap_keys128(const WideMap &w, const uint64_t *keys, uint64_t *out2, uint64_t n, cudaStream_t s);
 
 }  // namespace gs

@@ -85,6 +85,13 @@ typedef struct {
     float *host_vals;
     uint64_t host_capacity;
     uint64_t max_chunk_nnz;   /* 0 = derive from the HBM budget                */
+    /* Words per output key: 0 or 1 = one uint64 (x_f << Y_nfbits | y_f); 2 =
+     * the same key in 128 bits, two uint64 per nonzero, low word first
+     * (host_keys then holds 2 * host_capacity words, device chunks 2 * n).
+     * Needed when X's free bits + Y's free bits exceed 64, where the
+     * reference truncates the key (include/gsparc/contraction_extra.cuh:149-151)
+     * and gsparc_sptc with one word returns GSPARC_EUNSUPPORTED. */
+    int key_words;
 } gsparc_sink;
 
 /* Statistics of one contraction (the reference prints these to stderr,
