@@ -75,7 +75,8 @@ class Stats(ctypes.Structure):
                 ("verified_nnz", ctypes.c_uint64), ("verified_products", ctypes.c_uint64),
                 ("verify_mismatch", ctypes.c_uint64), ("verify_skipped_rows", ctypes.c_uint64),
                 ("max_rel_err", ctypes.c_double), ("max_abs_err", ctypes.c_double),
-                ("x_parts", ctypes.c_uint64), ("y_parts", ctypes.c_uint64)]
+                ("x_parts", ctypes.c_uint64), ("y_parts", ctypes.c_uint64),
+                ("kept_bitmap_bytes", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -85,7 +86,8 @@ _lib = None
 
 EXPORTS = [
     "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create", "gsparc_ctx_reserve",
-    "gsparc_ctx_set_verify", "gsparc_ctx_set_tiles", "gsparc_host_pin", "gsparc_host_unpin",
+    "gsparc_ctx_set_verify", "gsparc_ctx_set_tiles", "gsparc_ctx_set_row_bitmaps", "gsparc_host_pin",
+    "gsparc_host_unpin",
     "gsparc_ctx_destroy", "gsparc_ctx_memory", "gsparc_tensor_upload", "gsparc_tensor_free",
     "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
     "gsparc_free_host", "gsparc_layout", "gsparc_plan_shards", "gsparc_linearize",
@@ -171,6 +173,7 @@ def lib():
     L.gsparc_ctx_reserve.argtypes = [P, U64]
     L.gsparc_ctx_set_verify.argtypes = [P, U64]
     L.gsparc_ctx_set_tiles.argtypes = [P, U64, ctypes.c_uint32]
+    L.gsparc_ctx_set_row_bitmaps.argtypes = [P, I]
     L.gsparc_host_pin.argtypes = [P, U64]
     L.gsparc_host_unpin.argtypes = [P]
     L.gsparc_ctx_destroy.argtypes = [P]
@@ -327,6 +330,11 @@ class Context:
         light_row_max products use the on-chip ESC (<= 2048), heavy windows hold
         at most heavy_window_cap outputs."""
         _check(lib().gsparc_ctx_set_tiles(self._h, light_row_max, heavy_window_cap), "ctx_set_tiles")
+
+    def set_row_bitmaps(self, on: bool = True):
+        """Keep heavy rows' column bitmaps from the symbolic to the numeric pass
+        (default on; results are identical either way)."""
+        _check(lib().gsparc_ctx_set_row_bitmaps(self._h, 1 if on else 0), "ctx_set_row_bitmaps")
 
     def set_verify(self, max_products: int):
         """FP64 verification of later contractions' outputs on the GPU (all rows

@@ -141,6 +141,14 @@ gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint
     });
 }
 
+gsparc_status gsparc_ctx_set_row_bitmaps(gsparc_ctx *ctx, int on) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        GS_REQUIRE(on == 0 || on == 1, GSPARC_EINVAL, "on must be 0 or 1");
+        ctx->keep_row_bitmaps = on;
+    });
+}
+
 gsparc_status gsparc_ctx_set_verify(gsparc_ctx *ctx, uint64_t max_products) {
     return guard([&] {
         GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
@@ -296,6 +304,7 @@ gsparc_status gsparc_sptc_shard(gsparc_ctx *ctx, const gsparc_tensor *X, const g
             st.t_numeric_kernel_ms = bst.t_numeric_kernel_ms;
             st.heavy_windows = bst.heavy_windows;
             st.stream_rows = bst.stream_rows;
+            st.kept_bitmap_bytes = bst.kept_bitmap_bytes;
             *stats = st;
         }
     });

@@ -151,6 +151,7 @@ void sptc_resident(gsparc_ctx *ctx, const gsparc_tensor *X, const gsparc_tensor 
         st.t_numeric_kernel_ms = bst.t_numeric_kernel_ms;
         st.heavy_windows = bst.heavy_windows;
         st.stream_rows = bst.stream_rows;
+        st.kept_bitmap_bytes = bst.kept_bitmap_bytes;
         *stats = st;
     }
     *out = z.release();

@@ -145,6 +145,7 @@ struct gsparc_ctx {
     uint64_t verify_budget = 0;          // FP64 verification of outputs (0: off)
     uint64_t light_row_max = 0;          // rows with at most this many products use the on-chip ESC (0: default)
     uint32_t heavy_window_cap = 0;       // heavy rows: outputs per window (0: the compiled capacity)
+    int keep_row_bitmaps = 1;            // heavy rows: the symbolic pass keeps column bitmaps for the numeric pass
 };
 
 struct gsparc_tensor {

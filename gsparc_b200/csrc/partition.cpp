@@ -273,6 +273,7 @@ void add_stats(gsparc_stats &acc, const gsparc_stats &s) {
     acc.t_total_ms += s.t_total_ms;
     acc.t_numeric_kernel_ms += s.t_numeric_kernel_ms;
     acc.heavy_windows += s.heavy_windows;
+    acc.kept_bitmap_bytes = std::max(acc.kept_bitmap_bytes, s.kept_bitmap_bytes);  // parts run one at a time
     acc.verified_nnz += s.verified_nnz;
     acc.verified_products += s.verified_products;
     acc.verify_mismatch += s.verify_mismatch;
@@ -348,6 +349,7 @@ void sptc_partitioned(gsparc_ctx *ctx, const gsparc_coo *X, const gsparc_coo *Y,
         st.t_numeric_kernel_ms = bst.t_numeric_kernel_ms;
         st.heavy_windows = bst.heavy_windows;
         st.stream_rows = bst.stream_rows;
+        st.kept_bitmap_bytes = bst.kept_bitmap_bytes;
         acc.chunks += bst.chunks;
         acc.kernel_launches += bst.kernel_launches;
         acc.bytes_h2d += bst.bytes_h2d;

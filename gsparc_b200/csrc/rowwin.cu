@@ -28,6 +28,14 @@
 // symbolic pass (steps A, B and 1 on RW_SYM-wide windows: it keeps neither
 // accumulators nor the word prefix) counts each row's outputs as the columns
 // whose bit it set first.
+//
+// Kept bitmaps: for a row whose column bitmap over its rank span costs at most
+// kKeepBitsPerProduct bits per product, the symbolic pass also stores the
+// bitmap of every window in HBM (windows aligned to the bitmap's words, the
+// words of skipped ranges cleared).  The numeric pass then marks nothing: each
+// window loads its words, takes the word prefix, ends exactly where the
+// kHeavyCap-th column is passed, and finds every run's part with that end, so
+// windows are full and no product is read twice.
 #include "blockops.cuh"
 #include "kernels.cuh"
 
@@ -223,6 +231,96 @@ struct ProdItem {
     float xv, yv;
 };
 
+// Step A for runs b0 .. b0+nb-1 of the row: the part of each run from its
+// cursor up to the first rank >= lim goes (uncompacted) to the seg arrays,
+// its end to a.pend when KEEP_PEND.  Returns the smallest rank >= lim this
+// thread saw (INF if none): the next window's start.
+template <bool KEEP_PEND>
+__device__ __forceinline__ uint32_t find_parts(const AccArgs &a, uint32_t b0, uint32_t nb, uint32_t lim,
+                                               uint32_t *seg_start, uint32_t *seg_off, uint32_t *seg_run,
+                                               uint32_t *seg_cut) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint32_t nextmin = INF;
+    if (nb <= (uint32_t)kGallopWarpRuns) {
+        // few runs, long parts: one warp per run, 32-way fan-out search
+        for (uint32_t k = warp; k < nb; k += NWARPS) {
+            const uint32_t i = b0 + k;
+            const uint32_t p = a.cursor[i];
+            const uint32_t e = a.pos[i] + a.cnt[i];
+            uint32_t pe = p, fr = INF;
+            if (p < e) pe = warp_gallop(a.yrank, p, e, lim, &fr);
+            if (lane == 0) {
+                seg_start[k] = p;
+                seg_off[k] = pe - p;
+                seg_run[k] = i;
+                seg_cut[k] = pe;
+                if (KEEP_PEND) a.pend[i] = pe;
+            }
+            nextmin = min(nextmin, fr);
+        }
+    } else {
+        // many runs, short parts: one thread per run, doubling then bisection
+        for (uint32_t k = tid; k < nb; k += T) {
+            const uint32_t i = b0 + k;
+            const uint32_t p = a.cursor[i];
+            const uint32_t e = a.pos[i] + a.cnt[i];
+            uint32_t pe = p, fr = INF;
+            if (p < e) pe = thread_gallop(a.yrank, p, e, lim, &fr);
+            seg_start[k] = p;
+            seg_off[k] = pe - p;
+            seg_run[k] = i;
+            seg_cut[k] = pe;
+            if (KEEP_PEND) a.pend[i] = pe;
+            nextmin = min(nextmin, fr);
+        }
+    }
+    return nextmin;
+}
+
+// Step 4: slot -> column table from the window's bitmap (nwu words from rank
+// W0; the word prefix wp is read into registers before the table overwrites
+// it), then coalesced writes of the window's `outputs` slots and their reset.
+// Words go to threads cyclically (word tid + q*T), so a dense stretch of the
+// bitmap spreads over many threads instead of a few.
+__device__ __forceinline__ void write_window(const AccArgs &a, const uint32_t *bits, uint32_t *wp, float *hi,
+                                             float *lo, uint32_t nwu, uint32_t outputs, uint32_t W0,
+                                             uint64_t out_pos, uint64_t xf_hi, const uint64_t *cols) {
+    const uint32_t tid = threadIdx.x;
+    uint32_t *ocol = wp;
+    uint32_t myw[WPT_MAX], myp[WPT_MAX];
+#pragma unroll
+    for (int q = 0; q < WPT_MAX; ++q) {
+        const uint32_t w = tid + (uint32_t)q * T;
+        myw[q] = w < nwu ? bits[w] : 0u;
+        myp[q] = w < nwu ? wp[w] : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < WPT_MAX; ++q) {
+        uint32_t bw = myw[q];
+        uint32_t slot = myp[q];
+        const uint32_t cbase = W0 + 32u * (tid + (uint32_t)q * T);
+        while (bw && slot < outputs) {
+            ocol[slot++] = cbase + (uint32_t)(__ffs(bw) - 1);
+            bw &= bw - 1;
+        }
+    }
+    __syncthreads();
+    // The stores stream past L2 so the output does not evict the Y operand.
+    for (uint32_t q = tid; q < outputs; q += T) {
+        const uint64_t o = out_pos + q;
+        const float v = hi[q] + lo[q];
+        if (o < a.out_cap) {
+            __stcs(a.out_keys + o, (unsigned long long)(xf_hi | cols[ocol[q]]));
+            __stcs(a.out_vals + o, v);
+        } else {
+            atomicOr(a.err, 4u);
+        }
+        hi[q] = 0.f;
+        lo[q] = 0.f;
+    }
+}
+
 template <bool NUMERIC>
 __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -236,13 +334,12 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
     float *seg_xv = reinterpret_cast<float *>(seg_cut + MAXR); // [MAXR]  (numeric) X value of each part
     float *hi = seg_xv + (NUMERIC ? MAXR : 0);                 // [CAP]   (numeric)
     float *lo = hi + CAP;                                      // [CAP]   (numeric)
-    uint32_t *ocol = wp;  // step 4 reuses the word prefix as the slot -> column table
+    // (step 4 reuses the word prefix wp as the slot -> column table)
     __shared__ uint32_t s_tmp[33];
     __shared__ uint32_t s_unit;
     __shared__ uint32_t s_cut;
 
     const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
     // outputs per window: the compiled capacity, or a smaller tile chosen at run time
     const uint32_t cap = (a.heavy_cap && a.heavy_cap < (uint32_t)CAP) ? a.heavy_cap : (uint32_t)CAP;
 
@@ -283,9 +380,108 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         uint64_t out_pos = NUMERIC ? (a.row_off[row] - a.chunk_base) : 0;
         uint32_t row_total = 0;
         const bool one_batch = xe - xs <= (uint32_t)MAXR;  // parts from step A stay in place
+        // words of the row's kept column bitmap (0: none, the windows mark their columns)
+        const uint32_t nwr = a.row_bmw ? a.row_bmw[row] : 0u;
+
+        if (NUMERIC && nwr) {
+            // ---- kept bitmap: windows are swept contiguously from the row's
+            // smallest rank; each loads its words (from a 16-byte aligned word,
+            // the ranks below R masked off), so nothing is marked and the window
+            // ends exactly after its cap-th column.
+            const uint32_t rb = a.row_rb[row];
+            const uint32_t *src = a.hbm + a.row_bmoff[row];
+            uint32_t R = R0;  // every column below R is written
+            for (;;) {
+                const uint32_t wo = ((R - rb) >> 7) << 2;
+                if (wo >= nwr) break;
+                const uint32_t W0 = rb + 32u * wo;
+                const uint32_t nw = min((uint32_t)NWORDS, nwr - wo);
+                const uint32_t skip = R - W0;  // < 128
+                __syncthreads();  // the previous window no longer reads bits, prefix or table
+                for (uint32_t w = tid; w < nw; w += T) {
+                    uint32_t v = src[wo + w];
+                    const uint32_t first = 32u * w;
+                    if (first < skip) v = skip - first >= 32u ? 0u : v & (FULL << (skip - first));
+                    bits[w] = v;
+                }
+                __syncthreads();
+                const uint32_t wpt = (nw + T - 1) / T;
+                const uint32_t w0 = (uint32_t)tid * wpt;
+                const uint32_t w1 = min(w0 + wpt, nw);
+                uint32_t loc = 0;
+                for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
+                uint32_t Dw;
+                uint32_t run = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
+                for (uint32_t w = w0; w < w1; ++w) {
+                    wp[w] = run;
+                    run += __popc(bits[w]);
+                }
+                uint32_t R1 = W0 + 32u * nw, outputs = Dw;
+                if (Dw == 0) {  // a gap wider than the window (Dw is the same in every thread)
+                    R = R1;
+                    continue;
+                }
+                if (Dw > cap) {
+                    for (uint32_t w = w0; w < w1; ++w) {
+                        if (wp[w] <= cap && cap < wp[w] + __popc(bits[w])) {
+                            const uint32_t b = __fns(bits[w], 0u, (int)(cap - wp[w] + 1));
+                            s_cut = W0 + 32u * w + b;
+                        }
+                    }
+                    __syncthreads();
+                    R1 = s_cut;
+                    outputs = cap;
+                }
+                __syncthreads();
+                for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
+                    const uint32_t nb = min((uint32_t)MAXR, xe - b0);
+                    find_parts<false>(a, b0, nb, R1, seg_start, seg_off, seg_run, seg_cut);
+                    __syncthreads();
+                    const uint32_t ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
+                    for (uint32_t k = tid; k < ns; k += T) seg_xv[k] = a.xval[seg_run[k]];
+                    __syncthreads();
+                    flat_for<ProdItem>(
+                        seg_start, seg_off, ns,
+                        [&](uint32_t k, uint32_t idx, ProdItem &it) {
+                            it.r = a.yrank[idx];
+                            it.yv = a.yval[idx];
+                            it.xv = seg_xv[k];
+                        },
+                        [&](uint32_t, uint32_t, const ProdItem &it) {
+                            const uint32_t c = it.r - W0;  // in [skip, 32*nw): parts end below R1
+                            const uint32_t w = c >> 5;
+                            const uint32_t slot =
+                                w < nw ? wp[w] + __popc(bits[w] & ((1u << (c & 31)) - 1u)) : outputs;
+                            if (slot < outputs) {
+                                const float pr = it.xv * it.yv;
+                                const float pe = fmaf(it.xv, it.yv, -pr);
+                                const float old = atomicAdd(&hi[slot], pr);
+                                float s, err;
+                                two_sum(old, pr, s, err);
+                                atomicAdd(&lo[slot], err + pe);
+                            } else {
+                                atomicOr(a.err, 4u);  // the kept bitmap disagrees with the runs
+                            }
+                        });
+                    __syncthreads();
+                    for (uint32_t k = tid; k < ns; k += T) a.cursor[seg_run[k]] = seg_cut[k];
+                    __syncthreads();
+                }
+                write_window(a, bits, wp, hi, lo, nw, outputs, W0, out_pos, xf_hi, cols);
+                if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
+                out_pos += outputs;
+                row_total += outputs;
+                R = R1;
+            }
+            __syncthreads();
+            for (uint32_t w = tid; w < (uint32_t)NWORDS; w += T) bits[w] = 0;  // marking starts from a clear bitmap
+            R0 = INF;  // the row is done
+        }
 
         while (R0 != INF) {
-            const uint32_t lim = R0 + rw;  // ranks < 2^31: no wrap
+            // a kept row's symbolic windows start on a word of its bitmap
+            const uint32_t W0 = (!NUMERIC && nwr) ? R0 - ((R0 - a.row_rb[row]) & 31u) : R0;
+            const uint32_t lim = W0 + rw;  // ranks < 2^31: no wrap
             const uint32_t nwu = rw >> 5;  // bitmap words in use
             uint32_t nextmin = INF;
             uint32_t ns = 0;
@@ -294,39 +490,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             // ---- A, B, 1: parts of every run inside the window, marked in the bitmap
             for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
                 const uint32_t nb = min((uint32_t)MAXR, xe - b0);
-                if (nb <= (uint32_t)kGallopWarpRuns) {
-                    // few runs, long parts: one warp per run, 32-way fan-out search
-                    for (uint32_t k = warp; k < nb; k += NWARPS) {
-                        const uint32_t i = b0 + k;
-                        const uint32_t p = a.cursor[i];
-                        const uint32_t e = a.pos[i] + a.cnt[i];
-                        uint32_t pe = p, fr = INF;
-                        if (p < e) pe = warp_gallop(a.yrank, p, e, lim, &fr);
-                        if (lane == 0) {
-                            seg_start[k] = p;
-                            seg_off[k] = pe - p;
-                            seg_run[k] = i;
-                            seg_cut[k] = pe;
-                            a.pend[i] = pe;
-                        }
-                        nextmin = min(nextmin, fr);
-                    }
-                } else {
-                    // many runs, short parts: one thread per run, doubling then bisection
-                    for (uint32_t k = tid; k < nb; k += T) {
-                        const uint32_t i = b0 + k;
-                        const uint32_t p = a.cursor[i];
-                        const uint32_t e = a.pos[i] + a.cnt[i];
-                        uint32_t pe = p, fr = INF;
-                        if (p < e) pe = thread_gallop(a.yrank, p, e, lim, &fr);
-                        seg_start[k] = p;
-                        seg_off[k] = pe - p;
-                        seg_run[k] = i;
-                        seg_cut[k] = pe;
-                        a.pend[i] = pe;
-                        nextmin = min(nextmin, fr);
-                    }
-                }
+                nextmin = min(nextmin, find_parts<true>(a, b0, nb, lim, seg_start, seg_off, seg_run, seg_cut));
                 __syncthreads();
                 ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
                 if (NUMERIC)
@@ -335,7 +499,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                     seg_start, seg_off, ns,
                     [&](uint32_t, uint32_t idx, RankItem &it) { it.r = a.yrank[idx]; },
                     [&](uint32_t, uint32_t, const RankItem &it) {
-                        const uint32_t c = it.r - R0;
+                        const uint32_t c = it.r - W0;
                         const uint32_t m = 1u << (c & 31);
                         if (!(bits[c >> 5] & m)) {
                             const uint32_t old = atomicOr(&bits[c >> 5], m);
@@ -365,9 +529,27 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
 
             if (!NUMERIC) {
                 row_total += Dw;
-                for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
+                if (nwr) {
+                    // keep the window's words in the row's bitmap (coalesced), clearing them here
+                    uint32_t *dst = a.hbm + a.row_bmoff[row];
+                    const uint32_t wo = (W0 - a.row_rb[row]) >> 5;
+                    for (uint32_t w = tid; w < nwu; w += T) {
+                        if (wo + w < nwr) dst[wo + w] = bits[w];
+                        bits[w] = 0;
+                    }
+                } else {
+                    for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
+                }
                 for (uint32_t i = xs + tid; i < xe; i += T) a.cursor[i] = a.pend[i];
                 R0 = block_min_u32<T>(nextmin, s_tmp);
+                if (nwr) {
+                    // the words up to the next window's (or the bitmap's end) hold no column
+                    uint32_t *dst = a.hbm + a.row_bmoff[row];
+                    const uint32_t rb = a.row_rb[row];
+                    const uint32_t from = ((W0 - rb) >> 5) + nwu;
+                    const uint32_t to = R0 == INF ? nwr : min(nwr, (R0 - rb) >> 5);
+                    for (uint32_t w = from + tid; w < to; w += T) dst[w] = 0u;
+                }
                 continue;
             }
 
@@ -432,44 +614,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                 __syncthreads();
             }
 
-            // ---- 4: slot -> column table, then coalesced writes of the window.
-            // The word prefix is read into registers before the table overwrites it.
-            // Words go to threads cyclically (word tid + q*T), so a dense stretch of
-            // the bitmap spreads over many threads instead of a few.
-            {
-                uint32_t myw[WPT_MAX], myp[WPT_MAX];
-#pragma unroll
-                for (int q = 0; q < WPT_MAX; ++q) {
-                    const uint32_t w = (uint32_t)tid + (uint32_t)q * T;
-                    myw[q] = w < nwu ? bits[w] : 0u;
-                    myp[q] = w < nwu ? wp[w] : 0u;
-                }
-                __syncthreads();
-#pragma unroll
-                for (int q = 0; q < WPT_MAX; ++q) {
-                    uint32_t bw = myw[q];
-                    uint32_t slot = myp[q];
-                    const uint32_t cbase = R0 + 32u * ((uint32_t)tid + (uint32_t)q * T);
-                    while (bw && slot < outputs) {
-                        ocol[slot++] = cbase + (uint32_t)(__ffs(bw) - 1);
-                        bw &= bw - 1;
-                    }
-                }
-                __syncthreads();
-                // The stores stream past L2 so the output does not evict the Y operand.
-                for (uint32_t q = tid; q < outputs; q += T) {
-                    const uint64_t o = out_pos + q;
-                    const float v = hi[q] + lo[q];
-                    if (o < a.out_cap) {
-                        __stcs(a.out_keys + o, (unsigned long long)(xf_hi | cols[ocol[q]]));
-                        __stcs(a.out_vals + o, v);
-                    } else {
-                        atomicOr(a.err, 4u);
-                    }
-                    hi[q] = 0.f;
-                    lo[q] = 0.f;
-                }
-            }
+            // ---- 4: slot -> column table, then coalesced writes of the window
+            write_window(a, bits, wp, hi, lo, nwu, outputs, R0, out_pos, xf_hi, cols);
             for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
             if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
             out_pos += outputs;
@@ -490,6 +636,46 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         }
         if (!NUMERIC && tid == 0) a.row_nnz[row] = row_total;
         __syncthreads();
+    }
+}
+
+// Rank span of every heavy row: a warp per row (grid-stride over H, whose
+// count is on the device); runs are sorted by rank, so a run's first and last
+// entries bound it.
+__global__ void k_hspan(const uint32_t *__restrict__ H, const uint64_t *__restrict__ nh,
+                        const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ pos,
+                        const uint32_t *__restrict__ cnt, const uint32_t *__restrict__ yrank,
+                        const uint64_t *__restrict__ row_prod, uint32_t *__restrict__ row_bmw,
+                        uint32_t *__restrict__ row_rb) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t n = *nh;
+    for (uint64_t k = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n; k += nwarps) {
+        const uint32_t row = H[k];
+        const uint32_t xs = row_start[row], xe = row_start[row + 1];
+        uint32_t mn = INF, mx = 0;
+        for (uint32_t i = xs + lane; i < xe; i += 32) {
+            const uint32_t c = cnt[i];
+            if (c) {
+                const uint32_t p = pos[i];
+                mn = min(mn, yrank[p]);
+                mx = max(mx, yrank[p + c - 1]);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = min(mn, __shfl_xor_sync(FULL, mn, o));
+            mx = max(mx, __shfl_xor_sync(FULL, mx, o));
+        }
+        if (lane == 0) {
+            uint32_t words = 0;
+            if (mn != INF) {
+                const uint64_t span = (uint64_t)mx - mn + 1;
+                if (span <= kKeepBitsPerProduct * row_prod[row]) words = (uint32_t)(((span + 127) >> 7) << 2);
+            }
+            row_bmw[row] = words;
+            row_rb[row] = mn;
+        }
     }
 }
 
@@ -525,6 +711,20 @@ void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s) {
         GS_CUDA(cudaFuncSetAttribute(k_rowwin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_rowwin<false><<<grid, T, sm, s>>>(a);
     }
+    count_launch();
+    GS_CUDA(cudaGetLastError());
+}
+
+void launch_heavy_spans(const uint32_t *H, const uint64_t *nh, uint64_t nh_max, uint64_t nrows_max,
+                        const uint32_t *row_start, const uint32_t *pos, const uint32_t *cnt,
+                        const uint32_t *yrank, const uint64_t *row_prod, uint32_t *row_bmw, uint32_t *row_rb,
+                        cudaStream_t s) {
+    if (nrows_max) GS_CUDA(cudaMemsetAsync(row_bmw, 0, sizeof(uint32_t) * nrows_max, s));
+    if (nh_max == 0) return;
+    constexpr int B = 256;
+    const uint64_t blocks = (nh_max * 32 + B - 1) / B;
+    k_hspan<<<(unsigned)std::min<uint64_t>(blocks, 4096), B, 0, s>>>(H, nh, row_start, pos, cnt, yrank, row_prod,
+                                                                     row_bmw, row_rb);
     count_launch();
     GS_CUDA(cudaGetLastError());
 }

@@ -127,6 +127,7 @@ typedef struct {
     double max_rel_err;         /* max |z - z64| / |z64| over checked z64 != 0   */
     double max_abs_err;         /* max |z - z64| over checked outputs            */
     uint64_t x_parts, y_parts;  /* operand parts (gsparc_sptc_host; 0 otherwise) */
+    uint64_t kept_bitmap_bytes; /* heavy rows' column bitmaps kept from the symbolic to the numeric pass */
 } gsparc_stats;
 
 /* ---- version / errors ---------------------------------------------------- */
@@ -156,6 +157,14 @@ gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes);
  * reference, whose ESC and dense kernels have fixed launch shapes
  * (include/gsparc/contraction.cuh:287-290,469-472). */
 gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint32_t heavy_window_cap);
+/* Column bitmaps of heavy rows kept from the symbolic to the numeric pass
+ * (on = 1, the default; 0 = every heavy window marks its columns from the
+ * products).  A row's bitmap is kept when it costs at most 32 bits per matched
+ * product and all kept bitmaps fit an eighth of the memory left; the bytes
+ * used are in gsparc_stats.kept_bitmap_bytes.  Results are identical either
+ * way.  No counterpart in the reference, whose ESC re-expands every product
+ * (include/gsparc/contraction.cuh:440-561). */
+gsparc_status gsparc_ctx_set_row_bitmaps(gsparc_ctx *ctx, int on);
 /* FP64 verification of every later contraction on this context: each output
  * chunk's values are compared, before delivery, with FP64 sums of their
  * matched products formed on the GPU, for all rows when a contraction has at
