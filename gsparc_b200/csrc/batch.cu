@@ -635,7 +635,7 @@ struct GroupPlan {
     DBuf<uint64_t> cols, xprefix, row_xf, sprefix, row_off;
     DBuf<uint16_t> row_job;
     DBuf<uint32_t> Hc;         // heavy rows grouped by chunk (several chunks only)
-    DBuf<uint32_t> hbm, row_bmw, row_rb;  // heavy rows' kept column bitmaps (may be empty)
+    DBuf<uint32_t> hbm, row_rb;  // heavy rows' kept column bitmaps (may be empty)
     DBuf<uint64_t> row_bmoff;
     DBuf<unsigned int> flags;  // error bits, work counter, windows swept, spare
     struct Chunk {
@@ -835,14 +835,17 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     DBuf<uint64_t> sprefix(A, nx + 1, s);
     DBuf<uint32_t> row_nnz(A, nxb, s);
     GS_CUDA(cudaMemsetAsync(row_nnz.get(), 0, 4 * nxb, s));
-    // heavy rows' kept column bitmaps: words per row, smallest rank, word offsets
+    // heavy rows' kept column bitmaps: words of every heavy row and of the
+    // dense ones only, their word offsets, each row's smallest rank
     const bool keep_bm = ctx->keep_row_bitmaps != 0;
-    DBuf<uint32_t> row_bmw, row_rb;
-    DBuf<uint64_t> row_bmoff;
+    DBuf<uint32_t> bm_w_all, bm_w_dense, row_rb;
+    DBuf<uint64_t> bm_off_all, bm_off_dense;
     if (keep_bm) {
-        row_bmw.reset(A, nxb, s);
+        bm_w_all.reset(A, nxb, s);
+        bm_w_dense.reset(A, nxb, s);
         row_rb.reset(A, nxb, s);
-        row_bmoff.reset(A, nx + 1, s);
+        bm_off_all.reset(A, nx + 1, s);
+        bm_off_dense.reset(A, nx + 1, s);
     }
     {
         DBuf<uint8_t> rflag(A, nxb, s);
@@ -914,8 +917,10 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
         count_launch();
         GS_CUDA(cudaGetLastError());
         if (keep_bm) {
-            launch_heavy_spans(H, cnts.get() + 3, nx, nx, row_start, pos, cnt, rank, row_prod, row_bmw, row_rb, s);
-            exclusive_scan_u32_to_u64(A, row_bmw, row_bmoff, nx, s);
+            launch_heavy_spans(H, cnts.get() + 3, nx, nx, row_start, pos, cnt, rank, row_prod, bm_w_all, bm_w_dense,
+                               row_rb, s);
+            exclusive_scan_u32_to_u64(A, bm_w_all, bm_off_all, nx, s);
+            exclusive_scan_u32_to_u64(A, bm_w_dense, bm_off_dense, nx, s);
         }
     }
     uint64_t hc_cnt[16];
@@ -924,8 +929,11 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     d2h(hc_cnt, cnts.get(), 16, s);
     d2h(jerr.data(), d_jerr.get(), g, s);
     d2h(&ir, xprefix.get() + nx, 1, s);
-    uint64_t bm_words = 0;
-    if (keep_bm) d2h(&bm_words, row_bmoff.get() + nx, 1, s);
+    uint64_t bm_words_all = 0, bm_words_dense = 0;
+    if (keep_bm) {
+        d2h(&bm_words_all, bm_off_all.get() + nx, 1, s);
+        d2h(&bm_words_dense, bm_off_dense.get() + nx, 1, s);
+    }
     GS_CUDA(cudaStreamSynchronize(s));
     const uint64_t nrows = hc_cnt[2], nh = hc_cnt[3], nu = hc_cnt[5], nsr = hc_cnt[7];
     if (nshards > 1) ir = hc_cnt[11];  // the shard's products
@@ -981,17 +989,31 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     aa.row_xi = row_xi;
     aa.err = ctx->d_flag;
     aa.heavy_cap = ctx->heavy_window_cap;
-    // Kept bitmaps take at most an eighth of the memory left: the rest is for
-    // the output chunks.  Otherwise every heavy row marks its windows.
+    // Kept bitmaps take at most an eighth of the memory left (the rest is for
+    // the output chunks): every heavy row's if they fit, else the dense rows'
+    // (at most kKeepBitsPerProduct bits per product), else none and every
+    // heavy row marks its windows.
     DBuf<uint32_t> hbm;
-    if (keep_bm && nh && bm_words && bm_words * 4 <= A.available() / 8) {
-        hbm.reset(A, bm_words, s);
-        aa.hbm = hbm;
-        aa.row_bmoff = row_bmoff;
-        aa.row_bmw = row_bmw;
-        aa.row_rb = row_rb;
-        bst.kept_bitmap_bytes += bm_words * 4;
+    DBuf<uint64_t> *bm_off = nullptr;
+    if (keep_bm && nh) {
+        const uint64_t room = A.available() / 8;
+        if (bm_words_all && bm_words_all * 4 <= room)
+            bm_off = &bm_off_all;
+        else if (bm_words_dense && bm_words_dense * 4 <= room)
+            bm_off = &bm_off_dense;
     }
+    if (bm_off) {
+        const uint64_t words = bm_off == &bm_off_all ? bm_words_all : bm_words_dense;
+        hbm.reset(A, words, s);
+        aa.hbm = hbm;
+        aa.row_bmoff = *bm_off;
+        aa.row_rb = row_rb;
+        bst.kept_bitmap_bytes += words * 4;
+    }
+    bm_w_all.release();
+    bm_w_dense.release();
+    if (bm_off != &bm_off_all) bm_off_all.release();
+    if (bm_off != &bm_off_dense) bm_off_dense.release();
     const int ghs = std::max(1, ctx->sm_count * heavy_blocks_per_sm(false));
     const int gh = std::max(1, ctx->sm_count * heavy_blocks_per_sm(true));
     const int gl = std::max(1, ctx->sm_count * light_blocks_per_sm());
@@ -1172,11 +1194,10 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
         keep->row_off = std::move(row_off);
         keep->row_job = std::move(row_job);
         keep->Hc = std::move(Hc);
-        if (aa.row_bmw) {  // kept bitmaps are part of what the numeric pass reads
+        if (bm_off) {  // kept bitmaps are part of what the numeric pass reads
             keep->hbm = std::move(hbm);
-            keep->row_bmw = std::move(row_bmw);
             keep->row_rb = std::move(row_rb);
-            keep->row_bmoff = std::move(row_bmoff);
+            keep->row_bmoff = std::move(*bm_off);
         }
         keep->chunks.clear();
         for (auto &c : chunks) keep->chunks.push_back({c.lu0, c.lu1, c.h0, c.h1, c.s0, c.s1, c.first, c.n});

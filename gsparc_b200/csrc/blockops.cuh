@@ -8,6 +8,20 @@ namespace dev {
 
 static __device__ __forceinline__ uint64_t shl(uint64_t v, int s) { return s >= 64 ? 0ull : (v << s); }
 
+// 16-byte global -> shared copy that holds no register while in flight
+// (cp.async, cached in L2 only); both addresses 16-byte aligned.
+static __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+static __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Asks L2 to fetch [gmem, gmem + bytes) ahead of use (address 16-byte
+// aligned, bytes a multiple of 16); no data comes back to the SM.
+static __device__ __forceinline__ void prefetch_l2(const void *gmem, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(gmem), "r"(bytes) : "memory");
+}
+
 static __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
     s = a + b;
     float bp = s - a;
@@ -60,6 +74,35 @@ __device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t *s_
     __syncthreads();
     *total = s_tmp[32];
     return s_tmp[warp] + x - v;
+}
+
+// Exclusive block max-scan of one value per thread (0 for thread 0).
+template <int THREADS>
+__device__ __forceinline__ uint32_t block_excl_max_u32(uint32_t v, uint32_t *s_tmp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    uint32_t ex = __shfl_up_sync(0xffffffffu, x, 1);  // max over the lanes before this one
+    if (lane == 0) ex = 0;
+    __syncthreads();
+    if (lane == 31) s_tmp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t z = lane < THREADS / 32 ? s_tmp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z = max(z, y);
+        }
+        const uint32_t zex = __shfl_up_sync(0xffffffffu, z, 1);
+        s_tmp[lane] = lane ? zex : 0u;  // max over the warps before
+    }
+    __syncthreads();
+    return max(s_tmp[warp], ex);
 }
 
 

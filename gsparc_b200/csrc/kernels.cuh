@@ -97,12 +97,12 @@ struct AccArgs {
     uint32_t ncols;            // distinct Y free indices (column ranks are < ncols)
     uint32_t heavy_cap;        // heavy rows: outputs per window (0 or > kHeavyCap: kHeavyCap)
     // heavy rows: column bitmaps the symbolic pass keeps for the numeric pass
-    // (row_bmw null: none kept).  A kept row's bitmap is row_bmw[row] words at
-    // hbm + row_bmoff[row], bit 0 = column rank row_rb[row], the row's smallest.
+    // (row_bmoff null: none kept).  A kept row's bitmap is the words
+    // [row_bmoff[row], row_bmoff[row+1]) of hbm (a multiple of 4; none: the
+    // row marks its windows), bit 0 = column rank row_rb[row], its smallest.
     uint32_t *hbm;
-    const uint64_t *row_bmoff;
-    const uint32_t *row_bmw;   // [nrows] words kept (multiple of 4; 0: the row is marked per window)
-    const uint32_t *row_rb;    // [nrows]
+    const uint64_t *row_bmoff;  // [nrows + 1]
+    const uint32_t *row_rb;     // [nrows]
     // symbolic output
     uint32_t *row_nnz;         // [nrows]
     // numeric output
@@ -142,14 +142,15 @@ __device__ __forceinline__ void row_job_params(const AccArgs &a, uint32_t row, i
 
 void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
 // For the heavy rows H[0..*nh) (nh on the device, at most nh_max): the words of
-// a column bitmap over the row's rank span (row_bmw, a multiple of 4) and its
-// smallest rank (row_rb), for rows whose bitmap holds at most kKeepBitsPerProduct
-// bits per product; other rows keep row_bmw = 0 (row_bmw is cleared first).
+// a column bitmap over the row's rank span (a multiple of 4) in w_all, and in
+// w_dense only for rows whose bitmap holds at most kKeepBitsPerProduct bits
+// per matched product; the row's smallest rank in row_rb.  Both word arrays
+// are cleared first (nrows_max entries), so other rows have 0 words.
 constexpr uint64_t kKeepBitsPerProduct = 32;
 void launch_heavy_spans(const uint32_t *H, const uint64_t *nh, uint64_t nh_max, uint64_t nrows_max,
                         const uint32_t *row_start, const uint32_t *pos, const uint32_t *cnt,
-                        const uint32_t *yrank, const uint64_t *row_prod, uint32_t *row_bmw, uint32_t *row_rb,
-                        cudaStream_t s);
+                        const uint32_t *yrank, const uint64_t *row_prod, uint32_t *w_all, uint32_t *w_dense,
+                        uint32_t *row_rb, cudaStream_t s);
 // numeric pass of single-run rows (their symbolic count is their product count)
 void launch_stream(const AccArgs &a, int grid, cudaStream_t s);
 int stream_blocks_per_sm();

@@ -29,13 +29,15 @@
 // accumulators nor the word prefix) counts each row's outputs as the columns
 // whose bit it set first.
 //
-// Kept bitmaps: for a row whose column bitmap over its rank span costs at most
-// kKeepBitsPerProduct bits per product, the symbolic pass also stores the
-// bitmap of every window in HBM (windows aligned to the bitmap's words, the
-// words of skipped ranges cleared).  The numeric pass then marks nothing: each
-// window loads its words, takes the word prefix, ends exactly where the
-// kHeavyCap-th column is passed, and finds every run's part with that end, so
-// windows are full and no product is read twice.
+// Kept bitmaps: when the column bitmaps of the heavy rows over their rank
+// spans fit the memory set aside for them (else those of the rows that cost at
+// most kKeepBitsPerProduct bits per product), the symbolic pass also stores
+// the bitmap of every window in HBM (windows aligned to the bitmap's words,
+// the words of skipped ranges cleared).  The numeric pass then marks nothing:
+// each window copies its words to shared memory (cp.async, the next window's
+// words prefetched into L2 meanwhile), takes the word prefix, ends exactly
+// where the kHeavyCap-th column is passed, and finds every run's part with
+// that end, so windows are full and no product is read twice.
 #include "blockops.cuh"
 #include "kernels.cuh"
 
@@ -381,7 +383,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         uint32_t row_total = 0;
         const bool one_batch = xe - xs <= (uint32_t)MAXR;  // parts from step A stay in place
         // words of the row's kept column bitmap (0: none, the windows mark their columns)
-        const uint32_t nwr = a.row_bmw ? a.row_bmw[row] : 0u;
+        const uint32_t nwr = a.row_bmoff ? (uint32_t)(a.row_bmoff[row + 1] - a.row_bmoff[row]) : 0u;
 
         if (NUMERIC && nwr) {
             // ---- kept bitmap: windows are swept contiguously from the row's
@@ -396,43 +398,65 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                 if (wo >= nwr) break;
                 const uint32_t W0 = rb + 32u * wo;
                 const uint32_t nw = min((uint32_t)NWORDS, nwr - wo);
-                const uint32_t skip = R - W0;  // < 128
+                const uint32_t skip = R - W0;  // < 128: ranks [W0, R) of words 0..3 are done
                 __syncthreads();  // the previous window no longer reads bits, prefix or table
-                for (uint32_t w = tid; w < nw; w += T) {
-                    uint32_t v = src[wo + w];
-                    const uint32_t first = 32u * w;
-                    if (first < skip) v = skip - first >= 32u ? 0u : v & (FULL << (skip - first));
-                    bits[w] = v;
-                }
+                for (uint32_t q = tid; q < (nw >> 2); q += T) cp_async16(bits + 4u * q, src + wo + 4u * q);
+                cp_async_wait_all();
                 __syncthreads();
-                const uint32_t wpt = (nw + T - 1) / T;
+                // word prefix: thread t owns wpt consecutive words (a multiple of
+                // 4, read and written as 16-byte vectors); thread 0 clears the
+                // done ranks in words 0..3 before any other thread reads them
+                const uint32_t wpt = ((nw + T - 1) / T + 3u) & ~3u;
                 const uint32_t w0 = (uint32_t)tid * wpt;
                 const uint32_t w1 = min(w0 + wpt, nw);
                 uint32_t loc = 0;
-                for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
+                for (uint32_t w = w0; w < w1; w += 4) {
+                    uint4 v = *reinterpret_cast<const uint4 *>(bits + w);
+                    if (w == 0 && skip) {
+                        v.x = skip >= 32u ? 0u : v.x & (FULL << skip);
+                        v.y = skip >= 64u ? 0u : (skip <= 32u ? v.y : v.y & (FULL << (skip - 32u)));
+                        v.z = skip >= 96u ? 0u : (skip <= 64u ? v.z : v.z & (FULL << (skip - 64u)));
+                        v.w = skip <= 96u ? v.w : v.w & (FULL << (skip - 96u));
+                        *reinterpret_cast<uint4 *>(bits) = v;
+                    }
+                    loc += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+                }
                 uint32_t Dw;
-                uint32_t run = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
-                for (uint32_t w = w0; w < w1; ++w) {
-                    wp[w] = run;
-                    run += __popc(bits[w]);
+                const uint32_t run0 = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
+                uint32_t run = run0;
+                for (uint32_t w = w0; w < w1; w += 4) {
+                    const uint4 v = *reinterpret_cast<const uint4 *>(bits + w);
+                    uint4 p;
+                    p.x = run;
+                    p.y = p.x + __popc(v.x);
+                    p.z = p.y + __popc(v.y);
+                    p.w = p.z + __popc(v.z);
+                    run = p.w + __popc(v.w);
+                    *reinterpret_cast<uint4 *>(wp + w) = p;
+                }
+                if (Dw > cap && run0 <= cap && cap < run) {
+                    // this thread holds the cut: its word holding the (cap+1)-th column
+                    for (uint32_t w = w0; w < w1; ++w) {
+                        const uint32_t pw = wp[w], bw = bits[w];
+                        if (pw <= cap && cap < pw + __popc(bw))
+                            s_cut = W0 + 32u * w + (uint32_t)__fns(bw, 0u, (int)(cap - pw + 1));
+                    }
                 }
                 uint32_t R1 = W0 + 32u * nw, outputs = Dw;
                 if (Dw == 0) {  // a gap wider than the window (Dw is the same in every thread)
                     R = R1;
                     continue;
                 }
+                __syncthreads();
                 if (Dw > cap) {
-                    for (uint32_t w = w0; w < w1; ++w) {
-                        if (wp[w] <= cap && cap < wp[w] + __popc(bits[w])) {
-                            const uint32_t b = __fns(bits[w], 0u, (int)(cap - wp[w] + 1));
-                            s_cut = W0 + 32u * w + b;
-                        }
-                    }
-                    __syncthreads();
                     R1 = s_cut;
                     outputs = cap;
                 }
-                __syncthreads();
+                if (tid == 0) {
+                    // the next window's words, fetched into L2 while this one is accumulated
+                    const uint32_t wn = ((R1 - rb) >> 7) << 2;
+                    if (wn < nwr) prefetch_l2(src + wn, 4u * min((uint32_t)NWORDS, nwr - wn));
+                }
                 for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
                     const uint32_t nb = min((uint32_t)MAXR, xe - b0);
                     find_parts<false>(a, b0, nb, R1, seg_start, seg_off, seg_run, seg_cut);
@@ -645,8 +669,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
 __global__ void k_hspan(const uint32_t *__restrict__ H, const uint64_t *__restrict__ nh,
                         const uint32_t *__restrict__ row_start, const uint32_t *__restrict__ pos,
                         const uint32_t *__restrict__ cnt, const uint32_t *__restrict__ yrank,
-                        const uint64_t *__restrict__ row_prod, uint32_t *__restrict__ row_bmw,
-                        uint32_t *__restrict__ row_rb) {
+                        const uint64_t *__restrict__ row_prod, uint32_t *__restrict__ w_all,
+                        uint32_t *__restrict__ w_dense, uint32_t *__restrict__ row_rb) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const uint64_t n = *nh;
@@ -667,13 +691,11 @@ __global__ void k_hspan(const uint32_t *__restrict__ H, const uint64_t *__restri
             mn = min(mn, __shfl_xor_sync(FULL, mn, o));
             mx = max(mx, __shfl_xor_sync(FULL, mx, o));
         }
-        if (lane == 0) {
-            uint32_t words = 0;
-            if (mn != INF) {
-                const uint64_t span = (uint64_t)mx - mn + 1;
-                if (span <= kKeepBitsPerProduct * row_prod[row]) words = (uint32_t)(((span + 127) >> 7) << 2);
-            }
-            row_bmw[row] = words;
+        if (lane == 0 && mn != INF) {
+            const uint64_t span = (uint64_t)mx - mn + 1;
+            const uint32_t words = (uint32_t)(((span + 127) >> 7) << 2);
+            w_all[row] = words;
+            w_dense[row] = span <= kKeepBitsPerProduct * row_prod[row] ? words : 0u;
             row_rb[row] = mn;
         }
     }
@@ -717,14 +739,17 @@ void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s) {
 
 void launch_heavy_spans(const uint32_t *H, const uint64_t *nh, uint64_t nh_max, uint64_t nrows_max,
                         const uint32_t *row_start, const uint32_t *pos, const uint32_t *cnt,
-                        const uint32_t *yrank, const uint64_t *row_prod, uint32_t *row_bmw, uint32_t *row_rb,
-                        cudaStream_t s) {
-    if (nrows_max) GS_CUDA(cudaMemsetAsync(row_bmw, 0, sizeof(uint32_t) * nrows_max, s));
+                        const uint32_t *yrank, const uint64_t *row_prod, uint32_t *w_all, uint32_t *w_dense,
+                        uint32_t *row_rb, cudaStream_t s) {
+    if (nrows_max) {
+        GS_CUDA(cudaMemsetAsync(w_all, 0, sizeof(uint32_t) * nrows_max, s));
+        GS_CUDA(cudaMemsetAsync(w_dense, 0, sizeof(uint32_t) * nrows_max, s));
+    }
     if (nh_max == 0) return;
     constexpr int B = 256;
     const uint64_t blocks = (nh_max * 32 + B - 1) / B;
     k_hspan<<<(unsigned)std::min<uint64_t>(blocks, 4096), B, 0, s>>>(H, nh, row_start, pos, cnt, yrank, row_prod,
-                                                                     row_bmw, row_rb);
+                                                                     w_all, w_dense, row_rb);
     count_launch();
     GS_CUDA(cudaGetLastError());
 }

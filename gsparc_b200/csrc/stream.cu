@@ -12,11 +12,14 @@
 // The products of all such rows of a chunk form one flat index space.  A CTA
 // takes a tile of kStreamTile consecutive products and stages, for the rows
 // the tile touches (at most kRowBatch at a time), their flat start, first Y
-// entry, X value, output slot and key prefix in shared memory; every thread
-// then maps its products to (row, offset) there, so an output costs two
-// coalesced loads of the Y entry (its sorted key, whose low Y_nfbits bits are
-// the output column y_f, and its value), with SU outputs' loads in flight per
-// thread, and coalesced writes of the output.
+// entry, X value, output slot and key prefix in shared memory, and the staged
+// row of every product of the tile (each row marks its first product, a block
+// max-scan carries the marks over the rest), so an output costs one shared
+// lookup and two coalesced loads of the Y entry (its sorted key, whose low
+// Y_nfbits bits are the output column y_f, and its value), with SU outputs'
+// loads in flight per thread, and coalesced writes of the output.
+#include <cstring>
+
 #include "blockops.cuh"
 #include "kernels.cuh"
 
@@ -45,6 +48,8 @@ constexpr int kRowBatch = 512;  // rows whose parameters are staged at once
 constexpr int SU = 4;           // outputs per thread with loads in flight
 
 __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
+    __shared__ __align__(16) uint16_t s_row[kStreamTile];  // staged row of every output of the tile
+    __shared__ uint32_t s_tmp[33];
     __shared__ uint64_t s_pre[kRowBatch + 1];  // flat start of every staged row (+ the end)
     __shared__ uint64_t s_xf[kRowBatch];       // x_f << Y_nfbits
     __shared__ uint64_t s_o0[kRowBatch];       // row's first slot in the chunk buffer
@@ -82,6 +87,34 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
             __syncthreads();
             const uint64_t b0 = t0 > s_pre[0] ? t0 : s_pre[0];
             const uint64_t b1 = t1 < s_pre[nb] ? t1 : s_pre[nb];
+            // Row of every output of [b0, b1) (at most kStreamTile): each
+            // staged row marks where it starts inside the range (the row
+            // holding b0 marks 0), then a max-scan carries the marks forward.
+            constexpr int PER = kStreamTile / ST;  // marks per thread, one 16-byte vector
+            static_assert(PER == 8, "one uint4 of u16 marks per thread");
+            *reinterpret_cast<uint4 *>(s_row + PER * tid) = make_uint4(0, 0, 0, 0);
+            __syncthreads();
+            for (uint32_t i = tid; i < nb; i += ST)
+                if (s_pre[i + 1] > b0 && s_pre[i] < b1 && s_pre[i + 1] > s_pre[i])
+                    s_row[(s_pre[i] > b0 ? s_pre[i] : b0) - b0] = (uint16_t)i;
+            __syncthreads();
+            {
+                uint4 v = *reinterpret_cast<const uint4 *>(s_row + PER * tid);
+                uint16_t m[PER];
+                memcpy(m, &v, sizeof(v));
+                uint32_t run = 0;
+#pragma unroll
+                for (int k = 0; k < PER; ++k) run = max(run, (uint32_t)m[k]);
+                run = block_excl_max_u32<ST>(run, s_tmp);
+#pragma unroll
+                for (int k = 0; k < PER; ++k) {
+                    run = max(run, (uint32_t)m[k]);
+                    m[k] = (uint16_t)run;
+                }
+                memcpy(&v, m, sizeof(v));
+                *reinterpret_cast<uint4 *>(s_row + PER * tid) = v;
+            }
+            __syncthreads();
             for (uint64_t tb = b0 + tid; tb < b1; tb += (uint64_t)ST * SU) {
                 uint32_t li[SU], pp[SU];
                 uint64_t yk[SU];
@@ -92,14 +125,7 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
                     li[u] = 0;
                     pp[u] = 0;
                     if (t < b1) {
-                        uint32_t lo = 0, hi = nb;  // largest i with s_pre[i] <= t
-                        while (hi - lo > 1) {
-                            const uint32_t mid = (lo + hi) >> 1;
-                            if (s_pre[mid] <= t)
-                                lo = mid;
-                            else
-                                hi = mid;
-                        }
+                        const uint32_t lo = s_row[t - b0];  // largest i with s_pre[i] <= t
                         li[u] = lo;
                         pp[u] = (uint32_t)(t - s_pre[lo]);
                         const uint32_t j = s_j0[lo] + pp[u];

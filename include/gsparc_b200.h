@@ -159,9 +159,10 @@ gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes);
 gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint32_t heavy_window_cap);
 /* Column bitmaps of heavy rows kept from the symbolic to the numeric pass
  * (on = 1, the default; 0 = every heavy window marks its columns from the
- * products).  A row's bitmap is kept when it costs at most 32 bits per matched
- * product and all kept bitmaps fit an eighth of the memory left; the bytes
- * used are in gsparc_stats.kept_bitmap_bytes.  Results are identical either
+ * products).  The bitmaps (one bit per column rank over each heavy row's
+ * span) of all heavy rows are kept when they fit an eighth of the memory left,
+ * else those of the rows costing at most 32 bits per matched product, else
+ * none; the bytes used are in gsparc_stats.kept_bitmap_bytes.  Results are identical either
  * way.  No counterpart in the reference, whose ESC re-expands every product
  * (include/gsparc/contraction.cuh:440-561). */
 gsparc_status gsparc_ctx_set_row_bitmaps(gsparc_ctx *ctx, int on);
