@@ -289,6 +289,7 @@ def batched_stream(args, device, sp, stream):
     from gsparc_b200 import synth
     inst = synth.batched_instances(args.mixed_count, seed=3, max_nnz=1_000_000)
     ctx = gb.Context(device)
+    ctx.reserve()  # the pool mapped once, as for the headline contraction
     ops = [(ctx.upload(X, stream=sp), ctx.upload(Y, stream=sp)) for X, Y, _, _ in inst]
     jobs = [(dx, dy, cx, cy) for (dx, dy), (_, _, cx, cy) in zip(ops, inst)]
     nnz = sum(X.nnz + Y.nnz for X, Y, _, _ in inst)
@@ -405,9 +406,9 @@ def served_stream(args, device, sp, stream):
                 if d > 0:
                     time.sleep(d)
                 tickets[i] = srv.submit(sx, sy, cx, cy, sink="discard")
-        # one untimed pass of the same paced stream (the server's memory pool
-        # grows to its working size there, as the plain form gets a warm-up
-        # pass), then the timed one
+        # one untimed pass of the same paced stream (the plain form gets a
+        # warm-up pass too; both map their memory pools before it), then the
+        # timed one
         for rep in range(2):
             srv.reset_stats()
             th = threading.Thread(target=client)
@@ -423,6 +424,7 @@ def served_stream(args, device, sp, stream):
 
     # plain form on the same arrivals: one contraction at a time, in order
     ctx = gb.Context(device, hbm_budget=budget)
+    ctx.reserve()
     ops = [(ctx.upload(X, stream=sp), ctx.upload(Y, stream=sp)) for X, Y, _, _ in inst]
     jobs = [(dx, dy, cx, cy) for (dx, dy), (_, _, cx, cy) in zip(ops, inst)]
     ir = sum(gb.sptc(ctx, dx, dy, cx, cy, 0, sink="discard", stream=sp).ir_nnz for dx, dy, cx, cy in jobs)

@@ -990,9 +990,9 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     aa.err = ctx->d_flag;
     aa.heavy_cap = ctx->heavy_window_cap;
     // Kept bitmaps take at most an eighth of the memory left (the rest is for
-    // the output chunks): every heavy row's if they fit, else the dense rows'
-    // (at most kKeepBitsPerProduct bits per product), else none and every
-    // heavy row marks its windows.
+    // the output chunks): those of the heavy rows of at most kKeepBitsMax bits
+    // per product if they fit, else of the dense rows (at most
+    // kKeepBitsPerProduct), else none; the other heavy rows mark their windows.
     DBuf<uint32_t> hbm;
     DBuf<uint64_t> *bm_off = nullptr;
     if (keep_bm && nh) {

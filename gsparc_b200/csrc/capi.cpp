@@ -160,21 +160,7 @@ gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes) {
     return guard([&] {
         GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
         DeviceScope ds(ctx->device);
-        uint64_t n = bytes ? std::min<uint64_t>(bytes, ctx->arena.budget()) : ctx->arena.budget();
-        n &= ~((uint64_t(1) << 21) - 1);  // whole 2 MiB pages
-        if (n == 0) return;
-        // one allocation the size of the reservation, freed at once: the pool
-        // keeps the mapped memory (its release threshold is unbounded)
-        cudaStream_t s = ctx->copy_stream;
-        void *p = nullptr;
-        cudaError_t e = cudaMallocFromPoolAsync(&p, n, ctx->arena.pool(), s);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            gs::fail(e == cudaErrorMemoryAllocation ? GSPARC_ENOMEM : GSPARC_ECUDA,
-                     std::string("reserving ") + std::to_string(n) + " B failed: " + cudaGetErrorString(e));
-        }
-        GS_CUDA(cudaFreeAsync(p, s));
-        GS_CUDA(cudaStreamSynchronize(s));
+        ctx->arena.reserve(bytes, ctx->copy_stream);
     });
 }
 

@@ -72,6 +72,11 @@ public:
     // its own budget); the pool outlives the arena.
     void init_shared(int device, cudaMemPool_t pool, uint64_t budget);
     void set_budget(uint64_t budget) { budget_ = budget; }
+    // Map `bytes` (whole 2 MiB pages; 0 = the budget) into the pool now and keep
+    // them there: one allocation of that size freed at once (the pool's release
+    // threshold is unbounded), so later allocations carve mapped memory instead
+    // of growing the pool in the middle of a contraction.
+    void reserve(uint64_t bytes, cudaStream_t s);
     void reset_peak() { peak_ = in_use_; }
     void *alloc(size_t bytes, cudaStream_t s);
     void free(void *p, cudaStream_t s);

@@ -142,11 +142,13 @@ __device__ __forceinline__ void row_job_params(const AccArgs &a, uint32_t row, i
 
 void launch_heavy(const AccArgs &a, bool numeric, int grid, cudaStream_t s);
 // For the heavy rows H[0..*nh) (nh on the device, at most nh_max): the words of
-// a column bitmap over the row's rank span (a multiple of 4) in w_all, and in
-// w_dense only for rows whose bitmap holds at most kKeepBitsPerProduct bits
-// per matched product; the row's smallest rank in row_rb.  Both word arrays
-// are cleared first (nrows_max entries), so other rows have 0 words.
+// a column bitmap over the row's rank span (a multiple of 4) in w_all for rows
+// whose bitmap holds at most kKeepBitsMax bits per matched product, and in
+// w_dense for those with at most kKeepBitsPerProduct; the row's smallest rank
+// in row_rb.  Both word arrays are cleared first (nrows_max entries), so other
+// rows have 0 words.
 constexpr uint64_t kKeepBitsPerProduct = 32;
+constexpr uint64_t kKeepBitsMax = 512;
 void launch_heavy_spans(const uint32_t *H, const uint64_t *nh, uint64_t nh_max, uint64_t nrows_max,
                         const uint32_t *row_start, const uint32_t *pos, const uint32_t *cnt,
                         const uint32_t *yrank, const uint64_t *row_prod, uint32_t *w_all, uint32_t *w_dense,

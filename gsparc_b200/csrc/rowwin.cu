@@ -29,15 +29,16 @@
 // accumulators nor the word prefix) counts each row's outputs as the columns
 // whose bit it set first.
 //
-// Kept bitmaps: when the column bitmaps of the heavy rows over their rank
-// spans fit the memory set aside for them (else those of the rows that cost at
-// most kKeepBitsPerProduct bits per product), the symbolic pass also stores
-// the bitmap of every window in HBM (windows aligned to the bitmap's words,
-// the words of skipped ranges cleared).  The numeric pass then marks nothing:
-// each window copies its words to shared memory (cp.async, the next window's
-// words prefetched into L2 meanwhile), takes the word prefix, ends exactly
-// where the kHeavyCap-th column is passed, and finds every run's part with
-// that end, so windows are full and no product is read twice.
+// Kept bitmaps: for the heavy rows whose column bitmap over their rank span
+// costs at most kKeepBitsMax bits per product (kKeepBitsPerProduct when memory
+// is short), the symbolic pass also stores the bitmap of every window in HBM
+// (windows aligned to the bitmap's words, the words of skipped ranges
+// cleared).  The numeric pass then marks nothing: each window copies its words
+// to shared memory (cp.async, the next window's words prefetched into L2
+// meanwhile), takes the word prefix, ends exactly where the kHeavyCap-th
+// column is passed, and finds every run's part with that end, so windows are
+// full and no product is read twice; the next window starts at the row's next
+// column, so gaps are skipped.
 #include "blockops.cuh"
 #include "kernels.cuh"
 
@@ -279,14 +280,23 @@ __device__ __forceinline__ uint32_t find_parts(const AccArgs &a, uint32_t b0, ui
     return nextmin;
 }
 
+// Row constants kept in shared memory rather than registers (the numeric
+// kernel runs at the register limit of two CTAs per SM).
+struct RowConst {
+    uint64_t xf_hi;         // x_f << Y_nfbits: the high part of every output key of the row
+    const uint64_t *cols;   // the row's job's column table (rank -> y_f)
+    const uint32_t *src;    // the row's kept bitmap (numeric)
+    uint32_t rb;            // rank of the kept bitmap's bit 0
+};
+
 // Step 4: slot -> column table from the window's bitmap (nwu words from rank
 // W0; the word prefix wp is read into registers before the table overwrites
-// it), then coalesced writes of the window's `outputs` slots and their reset.
-// Words go to threads cyclically (word tid + q*T), so a dense stretch of the
-// bitmap spreads over many threads instead of a few.
+// it), then coalesced writes of the window's `outputs` outputs and the reset
+// of their accumulators.  Words go to threads cyclically (word tid + q*T), so
+// a dense stretch of the bitmap spreads over many threads instead of a few.
 __device__ __forceinline__ void write_window(const AccArgs &a, const uint32_t *bits, uint32_t *wp, float *hi,
                                              float *lo, uint32_t nwu, uint32_t outputs, uint32_t W0,
-                                             uint64_t out_pos, uint64_t xf_hi, const uint64_t *cols) {
+                                             uint32_t out_pos, const RowConst &rc) {
     const uint32_t tid = threadIdx.x;
     uint32_t *ocol = wp;
     uint32_t myw[WPT_MAX], myp[WPT_MAX];
@@ -309,8 +319,10 @@ __device__ __forceinline__ void write_window(const AccArgs &a, const uint32_t *b
     }
     __syncthreads();
     // The stores stream past L2 so the output does not evict the Y operand.
+    const uint64_t xf_hi = rc.xf_hi;
+    const uint64_t *cols = rc.cols;
     for (uint32_t q = tid; q < outputs; q += T) {
-        const uint64_t o = out_pos + q;
+        const uint64_t o = (uint64_t)out_pos + q;
         const float v = hi[q] + lo[q];
         if (o < a.out_cap) {
             __stcs(a.out_keys + o, (unsigned long long)(xf_hi | cols[ocol[q]]));
@@ -324,7 +336,7 @@ __device__ __forceinline__ void write_window(const AccArgs &a, const uint32_t *b
 }
 
 template <bool NUMERIC>
-__global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
+__global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // numeric: two CTAs per SM, symbolic: three
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NWK = NUMERIC ? NWORDS : NWORDS_SYM;
     uint32_t *bits = reinterpret_cast<uint32_t *>(smem_raw);  // [NWK]
@@ -340,6 +352,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
     __shared__ uint32_t s_tmp[33];
     __shared__ uint32_t s_unit;
     __shared__ uint32_t s_cut;
+    __shared__ uint32_t s_next;  // kept bitmaps: the smallest rank past the window (atomicMin)
+    __shared__ RowConst s_rc;
 
     const int tid = threadIdx.x;
     // outputs per window: the compiled capacity, or a smaller tile chosen at run time
@@ -357,11 +371,20 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
         if (u >= a.nunits) break;
         const uint32_t row = a.units[u];
         const uint32_t xs = a.row_start[row], xe = a.row_start[row + 1];
-        int y_nfbits;
-        const uint64_t *cols;
-        uint32_t ncols;
-        row_job_params(a, row, y_nfbits, cols, ncols);
-        const uint64_t xf_hi = shl(a.row_xf[row], y_nfbits);
+        // words of the row's kept column bitmap (0: none, the windows mark their columns)
+        const uint32_t nwr = a.row_bmoff ? (uint32_t)(a.row_bmoff[row + 1] - a.row_bmoff[row]) : 0u;
+        if (tid == 0) {  // read after the barriers of block_min_u32 below
+            int y_nfbits;
+            const uint64_t *cols;
+            uint32_t ncols;
+            row_job_params(a, row, y_nfbits, cols, ncols);
+            s_rc.xf_hi = shl(a.row_xf[row], y_nfbits);
+            s_rc.cols = cols;
+            if (nwr) {
+                s_rc.src = a.hbm + a.row_bmoff[row];
+                s_rc.rb = a.row_rb[row];
+            }
+        }
 
         uint32_t mymin = INF;
         for (uint32_t i = xs + tid; i < xe; i += T) {
@@ -373,35 +396,39 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
 
         // initial window width from the row's density (products vs columns)
         uint32_t rw = NUMERIC ? RW : RW_SYM;
-        if (NUMERIC) {
+        if (NUMERIC && !nwr) {
             const uint64_t P = a.xprefix[xe] - a.xprefix[xs];
+            int y_nfbits;
+            const uint64_t *cols;
+            uint32_t ncols;
+            row_job_params(a, row, y_nfbits, cols, ncols);
             const uint64_t est = (uint64_t)cap * ncols / (P ? P : 1);
             const uint64_t clamped = est < 32ull ? 32ull : (est > (uint64_t)RW ? (uint64_t)RW : est);
             rw = (uint32_t)clamped & ~31u;
         }
-        uint64_t out_pos = NUMERIC ? (a.row_off[row] - a.chunk_base) : 0;
+        // the row's first slot in the chunk buffer (a chunk holds fewer than 2^32 outputs)
+        uint32_t out_pos = NUMERIC ? (uint32_t)(a.row_off[row] - a.chunk_base) : 0u;
         uint32_t row_total = 0;
         const bool one_batch = xe - xs <= (uint32_t)MAXR;  // parts from step A stay in place
-        // words of the row's kept column bitmap (0: none, the windows mark their columns)
-        const uint32_t nwr = a.row_bmoff ? (uint32_t)(a.row_bmoff[row + 1] - a.row_bmoff[row]) : 0u;
 
         if (NUMERIC && nwr) {
             // ---- kept bitmap: windows are swept contiguously from the row's
             // smallest rank; each loads its words (from a 16-byte aligned word,
             // the ranks below R masked off), so nothing is marked and the window
             // ends exactly after its cap-th column.
-            const uint32_t rb = a.row_rb[row];
-            const uint32_t *src = a.hbm + a.row_bmoff[row];
             uint32_t R = R0;  // every column below R is written
             for (;;) {
+                const uint32_t rb = s_rc.rb;
+                if (R == INF) break;
                 const uint32_t wo = ((R - rb) >> 7) << 2;
                 if (wo >= nwr) break;
                 const uint32_t W0 = rb + 32u * wo;
                 const uint32_t nw = min((uint32_t)NWORDS, nwr - wo);
                 const uint32_t skip = R - W0;  // < 128: ranks [W0, R) of words 0..3 are done
-                __syncthreads();  // the previous window no longer reads bits, prefix or table
-                for (uint32_t q = tid; q < (nw >> 2); q += T) cp_async16(bits + 4u * q, src + wo + 4u * q);
+                __syncthreads();  // the previous window no longer reads bits, prefix, table or s_next
+                for (uint32_t q = tid; q < (nw >> 2); q += T) cp_async16(bits + 4u * q, s_rc.src + wo + 4u * q);
                 cp_async_wait_all();
+                if (tid == 0) s_next = INF;
                 __syncthreads();
                 // word prefix: thread t owns wpt consecutive words (a multiple of
                 // 4, read and written as 16-byte vectors); thread 0 clears the
@@ -426,7 +453,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                 uint32_t run = run0;
                 for (uint32_t w = w0; w < w1; w += 4) {
                     const uint4 v = *reinterpret_cast<const uint4 *>(bits + w);
-                    uint4 p;
+                    uint4 p;  // slots of the words' first columns
                     p.x = run;
                     p.y = p.x + __popc(v.x);
                     p.z = p.y + __popc(v.y);
@@ -455,11 +482,12 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                 if (tid == 0) {
                     // the next window's words, fetched into L2 while this one is accumulated
                     const uint32_t wn = ((R1 - rb) >> 7) << 2;
-                    if (wn < nwr) prefetch_l2(src + wn, 4u * min((uint32_t)NWORDS, nwr - wn));
+                    if (wn < nwr) prefetch_l2(s_rc.src + wn, 4u * min((uint32_t)NWORDS, nwr - wn));
                 }
                 for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
                     const uint32_t nb = min((uint32_t)MAXR, xe - b0);
-                    find_parts<false>(a, b0, nb, R1, seg_start, seg_off, seg_run, seg_cut);
+                    const uint32_t nm = find_parts<false>(a, b0, nb, R1, seg_start, seg_off, seg_run, seg_cut);
+                    if (nm != INF) atomicMin(&s_next, nm);
                     __syncthreads();
                     const uint32_t ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
                     for (uint32_t k = tid; k < ns; k += T) seg_xv[k] = a.xval[seg_run[k]];
@@ -480,8 +508,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                                 const float pr = it.xv * it.yv;
                                 const float pe = fmaf(it.xv, it.yv, -pr);
                                 const float old = atomicAdd(&hi[slot], pr);
-                                float s, err;
-                                two_sum(old, pr, s, err);
+                                float sum, err;
+                                two_sum(old, pr, sum, err);
                                 atomicAdd(&lo[slot], err + pe);
                             } else {
                                 atomicOr(a.err, 4u);  // the kept bitmap disagrees with the runs
@@ -491,11 +519,12 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                     for (uint32_t k = tid; k < ns; k += T) a.cursor[seg_run[k]] = seg_cut[k];
                     __syncthreads();
                 }
-                write_window(a, bits, wp, hi, lo, nw, outputs, W0, out_pos, xf_hi, cols);
+                write_window(a, bits, wp, hi, lo, nw, outputs, W0, out_pos, s_rc);
                 if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
                 out_pos += outputs;
                 row_total += outputs;
-                R = R1;
+                // the next window starts at the row's next column (skipping a gap; INF: none left)
+                R = max(R1, s_next);
             }
             __syncthreads();
             for (uint32_t w = tid; w < (uint32_t)NWORDS; w += T) bits[w] = 0;  // marking starts from a clear bitmap
@@ -582,8 +611,9 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             uint32_t R1 = lim, outputs = Dw;
             if (over) {
                 for (uint32_t w = w0; w < w1; ++w) {
-                    if (wp[w] <= cap && cap < wp[w] + __popc(bits[w])) {
-                        const uint32_t b = __fns(bits[w], 0u, (int)(cap - wp[w] + 1));
+                    const uint32_t pw = wp[w];
+                    if (pw <= cap && cap < pw + __popc(bits[w])) {
+                        const uint32_t b = __fns(bits[w], 0u, (int)(cap - pw + 1));
                         s_cut = R0 + 32u * w + b;
                     }
                 }
@@ -626,8 +656,8 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
                             const float pr = it.xv * it.yv;
                             const float pe = fmaf(it.xv, it.yv, -pr);
                             const float old = atomicAdd(&hi[slot], pr);
-                            float s, err;
-                            two_sum(old, pr, s, err);
+                            float sum, err;
+                            two_sum(old, pr, sum, err);
                             atomicAdd(&lo[slot], err + pe);
                         } else {
                             atomicMin(&seg_cut[k], idx);
@@ -639,7 +669,7 @@ __global__ void __launch_bounds__(T) k_rowwin(AccArgs a) {
             }
 
             // ---- 4: slot -> column table, then coalesced writes of the window
-            write_window(a, bits, wp, hi, lo, nwu, outputs, R0, out_pos, xf_hi, cols);
+            write_window(a, bits, wp, hi, lo, nwu, outputs, R0, out_pos, s_rc);
             for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
             if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
             out_pos += outputs;
@@ -694,7 +724,7 @@ __global__ void k_hspan(const uint32_t *__restrict__ H, const uint64_t *__restri
         if (lane == 0 && mn != INF) {
             const uint64_t span = (uint64_t)mx - mn + 1;
             const uint32_t words = (uint32_t)(((span + 127) >> 7) << 2);
-            w_all[row] = words;
+            w_all[row] = span <= kKeepBitsMax * row_prod[row] ? words : 0u;
             w_dense[row] = span <= kKeepBitsPerProduct * row_prod[row] ? words : 0u;
             row_rb[row] = mn;
         }

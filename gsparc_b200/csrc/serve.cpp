@@ -372,6 +372,11 @@ gsparc_status gsparc_serve_create(int device, const gsparc_server_opts *opts, gs
         S->budget = S->opt.hbm_budget_bytes ? S->opt.hbm_budget_bytes : (uint64_t)(fr * 0.9);
         S->resident.init(device, S->budget);
         GS_CUDA(cudaStreamCreateWithFlags(&S->up_stream, cudaStreamNonBlocking));
+        // the budget is mapped into the shared pool once, before any request:
+        // the lanes' working buffers (output chunks, kept row bitmaps) come and
+        // go in sizes that change with every batch, and growing the pool for
+        // one of them in the middle of a batch costs far more than the batch
+        S->resident.reserve(0, S->up_stream);
         int sms = 148;
         GS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         for (int i = 0; i < S->opt.lanes; ++i) {

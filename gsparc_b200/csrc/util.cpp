@@ -80,6 +80,21 @@ void Arena::init(int device, uint64_t budget) {
     GS_CUDA(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &thr));
 }
 
+void Arena::reserve(uint64_t bytes, cudaStream_t s) {
+    uint64_t n = bytes ? std::min<uint64_t>(bytes, budget_) : budget_;
+    n &= ~((uint64_t(1) << 21) - 1);
+    if (n == 0) return;
+    void *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, n, pool_, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(e == cudaErrorMemoryAllocation ? GSPARC_ENOMEM : GSPARC_ECUDA,
+             std::string("reserving ") + std::to_string(n) + " B failed: " + cudaGetErrorString(e));
+    }
+    GS_CUDA(cudaFreeAsync(p, s));
+    GS_CUDA(cudaStreamSynchronize(s));
+}
+
 void Arena::init_shared(int device, cudaMemPool_t pool, uint64_t budget) {
     device_ = device;
     budget_ = budget;

@@ -160,9 +160,10 @@ gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint
 /* Column bitmaps of heavy rows kept from the symbolic to the numeric pass
  * (on = 1, the default; 0 = every heavy window marks its columns from the
  * products).  The bitmaps (one bit per column rank over each heavy row's
- * span) of all heavy rows are kept when they fit an eighth of the memory left,
- * else those of the rows costing at most 32 bits per matched product, else
- * none; the bytes used are in gsparc_stats.kept_bitmap_bytes.  Results are identical either
+ * span) of the heavy rows costing at most 512 bits per matched product are
+ * kept when they fit an eighth of the memory left, else those costing at most
+ * 32 bits, else none; the bytes used are in gsparc_stats.kept_bitmap_bytes.
+ * Results are identical either
  * way.  No counterpart in the reference, whose ESC re-expands every product
  * (include/gsparc/contraction.cuh:440-561). */
 gsparc_status gsparc_ctx_set_row_bitmaps(gsparc_ctx *ctx, int on);
@@ -339,7 +340,9 @@ gsparc_status gsparc_tensor_set_values(gsparc_ctx *ctx, gsparc_tensor *t, const 
  * queued behind a large one that arrived just before it.  A request whose
  * output does not fit the HBM
  * budget streams it in chunks like gsparc_sptc.  Submit, poll, wait, stats
- * and upload may be called from any thread. */
+ * and upload may be called from any thread.  gsparc_serve_create maps the
+ * whole budget into the server's memory pool once (as gsparc_ctx_reserve
+ * does for a context), so no batch waits for the pool to grow. */
 typedef struct gsparc_server gsparc_server;
 
 typedef struct {
