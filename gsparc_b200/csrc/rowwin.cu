@@ -151,6 +151,35 @@ __device__ __forceinline__ void block_scan_inplace(uint32_t *v, uint32_t n, uint
 // the total at seg_off[ns].  Returns ns, the number of non-empty parts.
 __device__ __forceinline__ uint32_t compact_parts(uint32_t nb, uint32_t *seg_start, uint32_t *seg_off,
                                                   uint32_t *seg_run, uint32_t *seg_cut, uint32_t *s_tmp) {
+    if (nb <= 32u) {
+        // at most 32 parts: warp 0 alone (a ballot and one shuffle scan)
+        if (threadIdx.x < 32) {
+            const uint32_t k = threadIdx.x;
+            uint32_t st = 0, len = 0, rn = 0, ct = 0;
+            if (k < nb) { st = seg_start[k]; len = seg_off[k]; rn = seg_run[k]; ct = seg_cut[k]; }
+            const uint32_t bal = __ballot_sync(FULL, len != 0u);
+            uint32_t x = len;  // empty parts (and lanes past nb) add nothing
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, x, o);
+                if (k >= (uint32_t)o) x += y;
+            }
+            __syncwarp();  // every lane has read its part before any is overwritten
+            if (len) {
+                const uint32_t at = __popc(bal & ((1u << k) - 1u));
+                seg_start[at] = st;
+                seg_off[at] = x - len;
+                seg_run[at] = rn;
+                seg_cut[at] = ct;
+            }
+            if (k == 31) {
+                seg_off[__popc(bal)] = x;
+                s_tmp[32] = __popc(bal);
+            }
+        }
+        __syncthreads();
+        return s_tmp[32];
+    }
     const uint32_t k0 = 2u * threadIdx.x, k1 = k0 + 1u;
     uint32_t s0 = 0, l0 = 0, r0 = 0, c0 = 0, s1 = 0, l1 = 0, r1 = 0, c1 = 0;
     if (k0 < nb) { s0 = seg_start[k0]; l0 = seg_off[k0]; r0 = seg_run[k0]; c0 = seg_cut[k0]; }
