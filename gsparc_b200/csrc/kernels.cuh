@@ -116,7 +116,7 @@ struct AccArgs {
 
 constexpr int kHeavyThreads = 512;
 constexpr int kHeavyRW = 1 << 17;  // column ranks covered by one window's touched bitmap
-constexpr int kHeavyCap = 7168;    // output slots (compensated accumulators) per window
+constexpr int kHeavyCap = 8192;    // output slots (compensated accumulators) per window
                                    // (sized so two CTAs fit one SM's shared memory)
 constexpr int kHeavyMaxRuns = 512;   // runs flattened per batch
 constexpr int kGallopWarpRuns = 64;  // up to this many runs per batch: one warp per run search

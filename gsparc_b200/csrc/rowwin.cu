@@ -53,7 +53,12 @@ constexpr int RW = kHeavyRW;
 constexpr int NWORDS = RW / 32;
 constexpr int CAP = kHeavyCap;
 constexpr int MAXR = kHeavyMaxRuns;
-constexpr int WPN = (NWORDS > CAP ? NWORDS : CAP) + 4;  // word prefix, later the slot -> column table
+// Numeric pass, words of the bitmap region: the bitmap (NWORDS words), then
+// the word prefix (16-bit for a kept row's window, whose prefixes past the
+// capacity are clamped, 32-bit for a marked window); step 4 then reuses the
+// region as the slot -> column table (CAP words).
+constexpr int AW = (2 * NWORDS > CAP ? 2 * NWORDS : CAP);
+static_assert(CAP < 65535, "kept windows hold 16-bit prefixes");
 constexpr int WPT_MAX = (NWORDS + T - 1) / T;
 constexpr int RW_SYM = 262144;              // symbolic windows: no accumulators or word prefix kept
 constexpr int NWORDS_SYM = RW_SYM / 32;
@@ -319,21 +324,23 @@ struct RowConst {
 };
 
 // Step 4: slot -> column table from the window's bitmap (nwu words from rank
-// W0; the word prefix wp is read into registers before the table overwrites
-// it), then coalesced writes of the window's `outputs` outputs and the reset
-// of their accumulators.  Words go to threads cyclically (word tid + q*T), so
-// a dense stretch of the bitmap spreads over many threads instead of a few.
-__device__ __forceinline__ void write_window(const AccArgs &a, const uint32_t *bits, uint32_t *wp, float *hi,
-                                             float *lo, uint32_t nwu, uint32_t outputs, uint32_t W0,
-                                             uint32_t out_pos, const RowConst &rc) {
+// W0 at A, their prefixes at A + NWORDS: 16-bit when P16, else 32-bit; read
+// into registers before the table overwrites the region), then coalesced
+// writes of the window's `outputs` outputs and the reset of their
+// accumulators.  Words go to threads cyclically (word tid + q*T), so a dense
+// stretch of the bitmap spreads over many threads instead of a few.
+template <bool P16>
+__device__ __forceinline__ void write_window(const AccArgs &a, uint32_t *A, float *hi, float *lo, uint32_t nwu,
+                                             uint32_t outputs, uint32_t W0, uint32_t out_pos, const RowConst &rc) {
     const uint32_t tid = threadIdx.x;
-    uint32_t *ocol = wp;
+    uint32_t *ocol = A;
+    const uint16_t *wp16 = reinterpret_cast<const uint16_t *>(A + NWORDS);
     uint32_t myw[WPT_MAX], myp[WPT_MAX];
 #pragma unroll
     for (int q = 0; q < WPT_MAX; ++q) {
         const uint32_t w = tid + (uint32_t)q * T;
-        myw[q] = w < nwu ? bits[w] : 0u;
-        myp[q] = w < nwu ? wp[w] : 0u;
+        myw[q] = w < nwu ? A[w] : 0u;
+        myp[q] = w < nwu ? (P16 ? (uint32_t)wp16[w] : A[NWORDS + w]) : 0u;
     }
     __syncthreads();
 #pragma unroll
@@ -368,16 +375,18 @@ template <bool NUMERIC>
 __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // numeric: two CTAs per SM, symbolic: three
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NWK = NUMERIC ? NWORDS : NWORDS_SYM;
-    uint32_t *bits = reinterpret_cast<uint32_t *>(smem_raw);  // [NWK]
-    uint32_t *wp = bits + NWK;                                 // [WPN] (numeric)
-    uint32_t *seg_start = wp + (NUMERIC ? WPN : 0);            // [MAXR]
+    // numeric: region A (AW words, see AW); symbolic: the bitmap alone
+    uint32_t *A = reinterpret_cast<uint32_t *>(smem_raw);
+    uint32_t *bits = A;                                        // [NWK] bitmap
+    uint32_t *wp = A + NWORDS;                                 // [NWORDS] word prefix (marked windows, numeric)
+    uint16_t *wp16 = reinterpret_cast<uint16_t *>(A + NWORDS); // [NWORDS] word prefix (kept rows, numeric)
+    uint32_t *seg_start = A + (NUMERIC ? AW : NWK);            // [MAXR]
     uint32_t *seg_off = seg_start + MAXR;                      // [MAXR + 4]
     uint32_t *seg_run = seg_off + MAXR + 4;                    // [MAXR]
     uint32_t *seg_cut = seg_run + MAXR;                        // [MAXR]
     float *seg_xv = reinterpret_cast<float *>(seg_cut + MAXR); // [MAXR]  (numeric) X value of each part
     float *hi = seg_xv + (NUMERIC ? MAXR : 0);                 // [CAP]   (numeric)
     float *lo = hi + CAP;                                      // [CAP]   (numeric)
-    // (step 4 reuses the word prefix wp as the slot -> column table)
     __shared__ uint32_t s_tmp[33];
     __shared__ uint32_t s_unit;
     __shared__ uint32_t s_cut;
@@ -459,43 +468,54 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
                 cp_async_wait_all();
                 if (tid == 0) s_next = INF;
                 __syncthreads();
-                // word prefix: thread t owns wpt consecutive words (a multiple of
-                // 4, read and written as 16-byte vectors); thread 0 clears the
-                // done ranks in words 0..3 before any other thread reads them
+                // word prefix: thread t owns wpt consecutive words (4 or 8, read as
+                // 16-byte vectors; thread 0 clears the done ranks of words 0..3
+                // and writes them back before any other thread reads them), the
+                // 16-bit prefixes are written 4 at a time (clamped: slots past
+                // the capacity are never used)
                 const uint32_t wpt = ((nw + T - 1) / T + 3u) & ~3u;
+                static_assert(NWORDS <= 8 * T, "at most 8 words per thread");
                 const uint32_t w0 = (uint32_t)tid * wpt;
                 const uint32_t w1 = min(w0 + wpt, nw);
-                uint32_t loc = 0;
-                for (uint32_t w = w0; w < w1; w += 4) {
-                    uint4 v = *reinterpret_cast<const uint4 *>(bits + w);
-                    if (w == 0 && skip) {
-                        v.x = skip >= 32u ? 0u : v.x & (FULL << skip);
-                        v.y = skip >= 64u ? 0u : (skip <= 32u ? v.y : v.y & (FULL << (skip - 32u)));
-                        v.z = skip >= 96u ? 0u : (skip <= 64u ? v.z : v.z & (FULL << (skip - 64u)));
-                        v.w = skip <= 96u ? v.w : v.w & (FULL << (skip - 96u));
-                        *reinterpret_cast<uint4 *>(bits) = v;
-                    }
-                    loc += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+                uint4 v0 = make_uint4(0u, 0u, 0u, 0u), v1 = make_uint4(0u, 0u, 0u, 0u);
+                if (w0 < w1) v0 = *reinterpret_cast<const uint4 *>(bits + w0);
+                if (w0 + 4u < w1) v1 = *reinterpret_cast<const uint4 *>(bits + w0 + 4u);
+                if (w0 == 0 && skip) {
+                    v0.x = skip >= 32u ? 0u : v0.x & (FULL << skip);
+                    v0.y = skip >= 64u ? 0u : (skip <= 32u ? v0.y : v0.y & (FULL << (skip - 32u)));
+                    v0.z = skip >= 96u ? 0u : (skip <= 64u ? v0.z : v0.z & (FULL << (skip - 64u)));
+                    v0.w = skip <= 96u ? v0.w : v0.w & (FULL << (skip - 96u));
+                    *reinterpret_cast<uint4 *>(bits) = v0;
                 }
+                const uint32_t loc = __popc(v0.x) + __popc(v0.y) + __popc(v0.z) + __popc(v0.w) + __popc(v1.x) +
+                                     __popc(v1.y) + __popc(v1.z) + __popc(v1.w);
                 uint32_t Dw;
                 const uint32_t run0 = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
-                uint32_t run = run0;
-                for (uint32_t w = w0; w < w1; w += 4) {
-                    const uint4 v = *reinterpret_cast<const uint4 *>(bits + w);
-                    uint4 p;  // slots of the words' first columns
-                    p.x = run;
-                    p.y = p.x + __popc(v.x);
-                    p.z = p.y + __popc(v.y);
-                    p.w = p.z + __popc(v.z);
-                    run = p.w + __popc(v.w);
-                    *reinterpret_cast<uint4 *>(wp + w) = p;
+                if (w0 < w1) {
+                    // four 16-bit prefixes per 8-byte store
+                    uint32_t p = run0;
+                    auto pack = [&](uint32_t x, uint32_t y) {
+                        const uint32_t a0 = min(p, 0xffffu);
+                        p += __popc(x);
+                        const uint32_t a1 = min(p, 0xffffu);
+                        p += __popc(y);
+                        return a0 | (a1 << 16);
+                    };
+                    const uint32_t h0 = pack(v0.x, v0.y);
+                    const uint32_t h1 = pack(v0.z, v0.w);
+                    *reinterpret_cast<uint2 *>(wp16 + w0) = make_uint2(h0, h1);
+                    if (w0 + 4u < w1) {
+                        const uint32_t h2 = pack(v1.x, v1.y);
+                        const uint32_t h3 = pack(v1.z, v1.w);
+                        *reinterpret_cast<uint2 *>(wp16 + w0 + 4u) = make_uint2(h2, h3);
+                    }
                 }
-                if (Dw > cap && run0 <= cap && cap < run) {
+                if (Dw > cap && run0 <= cap && cap < run0 + loc) {
                     // this thread holds the cut: its word holding the (cap+1)-th column
                     for (uint32_t w = w0; w < w1; ++w) {
-                        const uint32_t pw = wp[w], bw = bits[w];
-                        if (pw <= cap && cap < pw + __popc(bw))
-                            s_cut = W0 + 32u * w + (uint32_t)__fns(bw, 0u, (int)(cap - pw + 1));
+                        const uint32_t pw = wp16[w], b = bits[w];
+                        if (pw <= cap && cap < pw + __popc(b))
+                            s_cut = W0 + 32u * w + (uint32_t)__fns(b, 0u, (int)(cap - pw + 1));
                     }
                 }
                 uint32_t R1 = W0 + 32u * nw, outputs = Dw;
@@ -532,7 +552,7 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
                             const uint32_t c = it.r - W0;  // in [skip, 32*nw): parts end below R1
                             const uint32_t w = c >> 5;
                             const uint32_t slot =
-                                w < nw ? wp[w] + __popc(bits[w] & ((1u << (c & 31)) - 1u)) : outputs;
+                                w < nw ? wp16[w] + __popc(bits[w] & ((1u << (c & 31)) - 1u)) : outputs;
                             if (slot < outputs) {
                                 const float pr = it.xv * it.yv;
                                 const float pe = fmaf(it.xv, it.yv, -pr);
@@ -548,15 +568,13 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
                     for (uint32_t k = tid; k < ns; k += T) a.cursor[seg_run[k]] = seg_cut[k];
                     __syncthreads();
                 }
-                write_window(a, bits, wp, hi, lo, nw, outputs, W0, out_pos, s_rc);
+                write_window<true>(a, A, hi, lo, nw, outputs, W0, out_pos, s_rc);
                 if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
                 out_pos += outputs;
                 row_total += outputs;
                 // the next window starts at the row's next column (skipping a gap; INF: none left)
                 R = max(R1, s_next);
             }
-            __syncthreads();
-            for (uint32_t w = tid; w < (uint32_t)NWORDS; w += T) bits[w] = 0;  // marking starts from a clear bitmap
             R0 = INF;  // the row is done
         }
 
@@ -568,6 +586,13 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
             uint32_t nextmin = INF;
             uint32_t ns = 0;
             uint32_t newcols = 0;  // symbolic: columns this thread marked first
+            if (NUMERIC) {
+                // the region held the previous window's table (or a kept row's pairs): clear the bitmap
+                __syncthreads();
+                for (uint32_t w = 4u * tid; w < (uint32_t)NWORDS; w += 4u * T)
+                    *reinterpret_cast<uint4 *>(bits + w) = make_uint4(0u, 0u, 0u, 0u);
+                __syncthreads();
+            }
 
             // ---- A, B, 1: parts of every run inside the window, marked in the bitmap
             for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
@@ -698,8 +723,7 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
             }
 
             // ---- 4: slot -> column table, then coalesced writes of the window
-            write_window(a, bits, wp, hi, lo, nwu, outputs, R0, out_pos, s_rc);
-            for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
+            write_window<false>(a, A, hi, lo, nwu, outputs, R0, out_pos, s_rc);
             if (tid == 0) atomicAdd(a.err + 2, 1u);  // windows swept (statistics)
             out_pos += outputs;
             row_total += outputs;
@@ -761,7 +785,7 @@ __global__ void k_hspan(const uint32_t *__restrict__ H, const uint64_t *__restri
 }
 
 size_t rowwin_smem(bool numeric) {
-    const size_t words = (numeric ? (size_t)NWORDS + WPN + MAXR : (size_t)NWORDS_SYM) + MAXR + (MAXR + 4) + MAXR + MAXR;
+    const size_t words = (numeric ? (size_t)AW + MAXR : (size_t)NWORDS_SYM) + MAXR + (MAXR + 4) + MAXR + MAXR;
     return words * 4 + (numeric ? (size_t)CAP * 8 : 0);
 }
 

@@ -152,8 +152,8 @@ gsparc_status gsparc_ctx_reserve(gsparc_ctx *ctx, uint64_t bytes);
 /* Tiles of the accumulation for later contractions on this context (0 = the
  * defaults): rows with at most light_row_max matched products (<= 2048,
  * default 1024) take the on-chip ESC, larger rows the windowed accumulator,
- * whose windows hold at most heavy_window_cap outputs (256..7168, default
- * 7168).  gsparc_autotune times candidates of both.  No counterpart in the
+ * whose windows hold at most heavy_window_cap outputs (256..8192, default
+ * 8192).  gsparc_autotune times candidates of both.  No counterpart in the
  * reference, whose ESC and dense kernels have fixed launch shapes
  * (include/gsparc/contraction.cuh:287-290,469-472). */
 gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint32_t heavy_window_cap);
