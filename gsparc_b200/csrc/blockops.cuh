@@ -76,6 +76,34 @@ __device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t *s_
     return s_tmp[warp] + x - v;
 }
 
+// Block sum of v and minimum of m, both returned to every thread, with two
+// barriers (s_tmp holds at least 2 * THREADS / 32 words).
+template <int THREADS>
+__device__ __forceinline__ void block_sum_min_u32(uint32_t v, uint32_t m, uint32_t *s_tmp, uint32_t &sum,
+                                                  uint32_t &mn) {
+    constexpr int NW = THREADS / 32;
+    static_assert(2 * NW <= 32, "sum and min of every warp fit s_tmp");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+        m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    __syncthreads();
+    if (lane == 0) {
+        s_tmp[warp] = v;
+        s_tmp[NW + warp] = m;
+    }
+    __syncthreads();
+    sum = 0;
+    mn = 0xffffffffu;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) {
+        sum += s_tmp[i];
+        mn = min(mn, s_tmp[NW + i]);
+    }
+}
+
 // Exclusive block max-scan of one value per thread (0 for thread 0).
 template <int THREADS>
 __device__ __forceinline__ uint32_t block_excl_max_u32(uint32_t v, uint32_t *s_tmp) {

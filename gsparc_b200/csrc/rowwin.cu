@@ -270,9 +270,12 @@ struct ProdItem {
 
 // Step A for runs b0 .. b0+nb-1 of the row: the part of each run from its
 // cursor up to the first rank >= lim goes (uncompacted) to the seg arrays,
-// its end to a.pend when KEEP_PEND.  Returns the smallest rank >= lim this
-// thread saw (INF if none): the next window's start.
-template <bool KEEP_PEND>
+// its end to a.pend (END_TO = 1: the marking numeric pass reads the parts
+// again) or straight to the run's cursor (END_TO = 2: the symbolic pass, which
+// reads them once), or nowhere (0: the caller moves the cursors itself).
+// Returns the smallest rank >= lim this thread saw (INF if none): the next
+// window's start.
+template <int END_TO>
 __device__ __forceinline__ uint32_t find_parts(const AccArgs &a, uint32_t b0, uint32_t nb, uint32_t lim,
                                                uint32_t *seg_start, uint32_t *seg_off, uint32_t *seg_run,
                                                uint32_t *seg_cut) {
@@ -291,7 +294,8 @@ __device__ __forceinline__ uint32_t find_parts(const AccArgs &a, uint32_t b0, ui
                 seg_off[k] = pe - p;
                 seg_run[k] = i;
                 seg_cut[k] = pe;
-                if (KEEP_PEND) a.pend[i] = pe;
+                if (END_TO == 1) a.pend[i] = pe;
+                if (END_TO == 2) a.cursor[i] = pe;
             }
             nextmin = min(nextmin, fr);
         }
@@ -307,7 +311,8 @@ __device__ __forceinline__ uint32_t find_parts(const AccArgs &a, uint32_t b0, ui
             seg_off[k] = pe - p;
             seg_run[k] = i;
             seg_cut[k] = pe;
-            if (KEEP_PEND) a.pend[i] = pe;
+            if (END_TO == 1) a.pend[i] = pe;
+            if (END_TO == 2) a.cursor[i] = pe;
             nextmin = min(nextmin, fr);
         }
     }
@@ -535,7 +540,7 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
                 }
                 for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
                     const uint32_t nb = min((uint32_t)MAXR, xe - b0);
-                    const uint32_t nm = find_parts<false>(a, b0, nb, R1, seg_start, seg_off, seg_run, seg_cut);
+                    const uint32_t nm = find_parts<0>(a, b0, nb, R1, seg_start, seg_off, seg_run, seg_cut);
                     if (nm != INF) atomicMin(&s_next, nm);
                     __syncthreads();
                     const uint32_t ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
@@ -579,8 +584,8 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
         }
 
         while (R0 != INF) {
-            // a kept row's symbolic windows start on a word of its bitmap
-            const uint32_t W0 = (!NUMERIC && nwr) ? R0 - ((R0 - a.row_rb[row]) & 31u) : R0;
+            // a kept row's symbolic windows start on a 16-byte boundary of its bitmap
+            const uint32_t W0 = (!NUMERIC && nwr) ? R0 - ((R0 - s_rc.rb) & 127u) : R0;
             const uint32_t lim = W0 + rw;  // ranks < 2^31: no wrap
             const uint32_t nwu = rw >> 5;  // bitmap words in use
             uint32_t nextmin = INF;
@@ -597,7 +602,7 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
             // ---- A, B, 1: parts of every run inside the window, marked in the bitmap
             for (uint32_t b0 = xs; b0 < xe; b0 += MAXR) {
                 const uint32_t nb = min((uint32_t)MAXR, xe - b0);
-                nextmin = min(nextmin, find_parts<true>(a, b0, nb, lim, seg_start, seg_off, seg_run, seg_cut));
+                nextmin = min(nextmin, find_parts<NUMERIC ? 1 : 2>(a, b0, nb, lim, seg_start, seg_off, seg_run, seg_cut));
                 __syncthreads();
                 ns = compact_parts(nb, seg_start, seg_off, seg_run, seg_cut, s_tmp);
                 if (NUMERIC)
@@ -616,48 +621,44 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
                 __syncthreads();
             }
 
+            if (!NUMERIC) {
+                // a kept row's window goes to its bitmap (16-byte pieces, coalesced);
+                // the bitmap is cleared for the next window either way
+                static_assert(NWORDS_SYM % (4 * T) == 0, "whole 16-byte pieces per thread");
+                uint32_t *dst = nwr ? a.hbm + a.row_bmoff[row] : nullptr;
+                const uint32_t wo = nwr ? (W0 - s_rc.rb) >> 5 : 0u;  // a multiple of 4
+                for (uint32_t q = 4u * tid; q < nwu; q += 4u * T) {
+                    if (nwr && wo + q < nwr)
+                        *reinterpret_cast<uint4 *>(dst + wo + q) = *reinterpret_cast<const uint4 *>(bits + q);
+                    *reinterpret_cast<uint4 *>(bits + q) = make_uint4(0u, 0u, 0u, 0u);
+                }
+                // the window's new columns and the next window's start (the run
+                // searches moved the cursors already)
+                uint32_t Dw;
+                block_sum_min_u32<T>(newcols, nextmin, s_tmp, Dw, R0);
+                row_total += Dw;
+                if (nwr) {
+                    // the words up to the next window's (or the bitmap's end) hold no column
+                    const uint32_t from = wo + nwu;
+                    const uint32_t to = R0 == INF ? nwr : min(nwr, ((R0 - s_rc.rb) >> 7) << 2);
+                    for (uint32_t q = from + 4u * tid; q < to; q += 4u * T)
+                        *reinterpret_cast<uint4 *>(dst + q) = make_uint4(0u, 0u, 0u, 0u);
+                }
+                continue;
+            }
+
             // ---- 2: word prefix of the bitmap
             // words in use are split in blocks of wpt consecutive words per thread
             const uint32_t wpt = (nwu + T - 1) / T;
             const uint32_t w0 = (uint32_t)tid * wpt;
             const uint32_t w1 = min(w0 + wpt, nwu);
             uint32_t loc = 0;
-            if (NUMERIC)
-                for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
-            else
-                loc = newcols;
+            for (uint32_t w = w0; w < w1; ++w) loc += __popc(bits[w]);
             uint32_t Dw;
             uint32_t run = block_excl_scan_u32<T>(loc, s_tmp, &Dw);
-            if (NUMERIC)
-                for (uint32_t w = w0; w < w1; ++w) {
-                    wp[w] = run;
-                    run += __popc(bits[w]);
-                }
-
-            if (!NUMERIC) {
-                row_total += Dw;
-                if (nwr) {
-                    // keep the window's words in the row's bitmap (coalesced), clearing them here
-                    uint32_t *dst = a.hbm + a.row_bmoff[row];
-                    const uint32_t wo = (W0 - a.row_rb[row]) >> 5;
-                    for (uint32_t w = tid; w < nwu; w += T) {
-                        if (wo + w < nwr) dst[wo + w] = bits[w];
-                        bits[w] = 0;
-                    }
-                } else {
-                    for (uint32_t w = w0; w < w1; ++w) bits[w] = 0;
-                }
-                for (uint32_t i = xs + tid; i < xe; i += T) a.cursor[i] = a.pend[i];
-                R0 = block_min_u32<T>(nextmin, s_tmp);
-                if (nwr) {
-                    // the words up to the next window's (or the bitmap's end) hold no column
-                    uint32_t *dst = a.hbm + a.row_bmoff[row];
-                    const uint32_t rb = a.row_rb[row];
-                    const uint32_t from = ((W0 - rb) >> 5) + nwu;
-                    const uint32_t to = R0 == INF ? nwr : min(nwr, (R0 - rb) >> 5);
-                    for (uint32_t w = from + tid; w < to; w += T) dst[w] = 0u;
-                }
-                continue;
+            for (uint32_t w = w0; w < w1; ++w) {
+                wp[w] = run;
+                run += __popc(bits[w]);
             }
 
             // ---- numeric: cut the window at the CAP-th touched column if needed
