@@ -51,12 +51,16 @@ WORKLOAD = "esc_large"
 METRIC = "matched products/sec"
 UNIT = "products/s"
 # ncu DRAM bytes (read + write) of the numeric launches (k_light<1>, k_rowwin<1>, k_stream) per output
-# nonzero, measured on esc_large at scale 0.1 (one output chunk, 2.50e8 outputs)
-TRAFFIC_NUMERIC_PER_OUTPUT = (28.42e6 + 2848.87e6) / 2.50473870e8
-# ncu DRAM bytes of every other kernel of a contraction (linearise, sort, match, planning, symbolic
-# pass) per operand nonzero (X + Y), same workload at scale 0.1 (310k + 310k operand nonzeros: 134.86 MB
-# read; their writes stay in L2 at that size)
-TRAFFIC_OTHER_PER_OPERAND_NNZ = 134.86e6 / 620000
+# nonzero, the kept bitmaps' reads left out, measured on esc_large at scale 0.1 (one output chunk,
+# 2.50e8 outputs: 307.70 MB read of which 268.27 MB kept bitmaps, 2858.71 MB written)
+TRAFFIC_NUMERIC_PER_OUTPUT = 2898.144436e6 / 2.50473870e8
+# kept heavy-row bitmaps: written by the symbolic pass (208.30 MB reach DRAM), read once by the numeric
+# pass (268.27 MB), per kept byte, same capture
+TRAFFIC_PER_KEPT_BITMAP_BYTE = 476.565904e6 / 268267904
+# ncu DRAM bytes of every other kernel of a contraction (linearise, sort, match, planning, spans,
+# symbolic pass reads) per operand nonzero (X + Y), same capture (310k + 310k operand nonzeros:
+# 144.67 MB read; their writes stay in L2 at that size)
+TRAFFIC_OTHER_PER_OPERAND_NNZ = 144.665904e6 / 620000
 
 
 def parse():
@@ -673,6 +677,7 @@ def ours_arm(args, world, rank, local, dist):
     alg = alg_bytes_contraction(X.nnz, X.order, X.nnz, X.order, ir, s0["nnz"])
     achieved = alg / (t_step / 1e3) / 1e9
     traffic = (TRAFFIC_NUMERIC_PER_OUTPUT * s0["nnz"]
+               + TRAFFIC_PER_KEPT_BITMAP_BYTE * s0["kept_bitmap_bytes"]
                + TRAFFIC_OTHER_PER_OPERAND_NNZ * (s0["nnz_x"] + s0["nnz_y"]))
     roofline = {"bound": "hbm", "kernel": "the contraction: linearise, sort, match, planning, symbolic and "
                 "numeric accumulation of every output chunk",
@@ -680,7 +685,8 @@ def ours_arm(args, world, rank, local, dist):
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                 "traffic": traffic,
                 "traffic_scope": "DRAM bytes read + written by every kernel of one contraction, from ncu "
-                                 "captures at scale 0.1 scaled per output (numeric kernels) and per operand "
+                                 "captures at scale 0.1 scaled per output (numeric kernels), per kept bitmap "
+                                 "byte (written by the symbolic pass, read by the numeric) and per operand "
                                  "nonzero (the rest)",
                 "alg_bytes": alg,
                 "alg_formula": "sum over X, Y of nnz*(8*order+4) + 24*nnz, + 16*nnz_X + 8*nnz_Y + 24*products "
