@@ -42,12 +42,30 @@ __device__ __forceinline__ uint64_t upper_bound_u64(const uint64_t *a, uint64_t 
     return lo;
 }
 
+// The first i in [lo, hi) with a[i] > v (hi if none), given a[lo] <= v: steps
+// of 1, 2, 4, ... forward from lo, then bisection of the last step, so a
+// target k entries past lo costs about 2*log2(k) loads.
+__device__ __forceinline__ uint64_t gallop_upper_u64(const uint64_t *a, uint64_t lo, uint64_t hi, uint64_t v) {
+    uint64_t b = lo, e = hi, step = 1;
+    for (;;) {
+        const uint64_t q = b + step;
+        if (q >= hi) break;
+        if (a[q] > v) {
+            e = q;
+            break;
+        }
+        b = q;
+        step <<= 1;
+    }
+    return upper_bound_u64(a, b + 1, e, v);
+}
+
 __device__ __forceinline__ uint64_t low_mask(int b) { return b >= 64 ? ~0ull : ((1ull << b) - 1); }
 
 constexpr int kRowBatch = 512;  // rows whose parameters are staged at once
 constexpr int SU = 4;           // outputs per thread with loads in flight
 
-__global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
+__global__ void __launch_bounds__(ST, 6) k_stream(AccArgs a) {
     __shared__ __align__(16) uint16_t s_row[kStreamTile];  // staged row of every output of the tile
     __shared__ uint32_t s_tmp[33];
     __shared__ uint64_t s_pre[kRowBatch + 1];  // flat start of every staged row (+ the end)
@@ -62,12 +80,20 @@ __global__ void __launch_bounds__(ST) k_stream(AccArgs a) {
     const uint64_t P0 = a.sprefix[0];
     const uint64_t total = a.sprefix[ns] - P0;
 
-    for (uint64_t t0 = (uint64_t)blockIdx.x * kStreamTile; t0 < total; t0 += (uint64_t)gridDim.x * kStreamTile) {
+    // a CTA takes a contiguous range of tiles, so each tile finds its rows by a
+    // short forward search from the previous tile's last row
+    const uint64_t ntiles = (total + kStreamTile - 1) / kStreamTile;
+    const uint64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
+    const uint64_t tile_e = min(ntiles, (uint64_t)(blockIdx.x + 1) * per);
+    uint64_t hint = 0;  // a row whose flat start is at or before this tile's first product
+    for (uint64_t tile = (uint64_t)blockIdx.x * per; tile < tile_e; ++tile) {
+        const uint64_t t0 = tile * kStreamTile;
         const uint64_t t1 = t0 + kStreamTile < total ? t0 + kStreamTile : total;
         // rows k0..k1 hold the tile's first and last product
-        if (tid < 2) s_k[tid] = upper_bound_u64(a.sprefix, 0, ns + 1, P0 + (tid ? t1 - 1 : t0)) - 1;
+        if (tid < 2) s_k[tid] = gallop_upper_u64(a.sprefix, hint, ns + 1, P0 + (tid ? t1 - 1 : t0)) - 1;
         __syncthreads();
         const uint64_t k0 = s_k[0], k1 = s_k[1];
+        hint = k1;
         for (uint64_t kb = k0; kb <= k1; kb += kRowBatch) {
             const uint32_t nb = (uint32_t)(k1 - kb + 1 < (uint64_t)kRowBatch ? k1 - kb + 1 : (uint64_t)kRowBatch);
             for (uint32_t i = tid; i <= nb; i += ST) s_pre[i] = a.sprefix[kb + i] - P0;
