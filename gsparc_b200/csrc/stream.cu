@@ -29,7 +29,7 @@ namespace {
 using namespace dev;
 
 constexpr int ST = 256;
-constexpr int kStreamTile = 2048;
+constexpr int kStreamTile = 4096;
 
 __device__ __forceinline__ uint64_t upper_bound_u64(const uint64_t *a, uint64_t lo, uint64_t hi, uint64_t v) {
     while (lo < hi) {
@@ -116,18 +116,23 @@ __global__ void __launch_bounds__(ST, 6) k_stream(AccArgs a) {
             // Row of every output of [b0, b1) (at most kStreamTile): each
             // staged row marks where it starts inside the range (the row
             // holding b0 marks 0), then a max-scan carries the marks forward.
-            constexpr int PER = kStreamTile / ST;  // marks per thread, one 16-byte vector
-            static_assert(PER == 8, "one uint4 of u16 marks per thread");
-            *reinterpret_cast<uint4 *>(s_row + PER * tid) = make_uint4(0, 0, 0, 0);
+            constexpr int PER = kStreamTile / ST;  // marks per thread, in 16-byte vectors
+            static_assert(PER % 8 == 0, "whole uint4s of u16 marks per thread");
+#pragma unroll
+            for (int c = 0; c < PER; c += 8)
+                *reinterpret_cast<uint4 *>(s_row + PER * tid + c) = make_uint4(0, 0, 0, 0);
             __syncthreads();
             for (uint32_t i = tid; i < nb; i += ST)
                 if (s_pre[i + 1] > b0 && s_pre[i] < b1 && s_pre[i + 1] > s_pre[i])
                     s_row[(s_pre[i] > b0 ? s_pre[i] : b0) - b0] = (uint16_t)i;
             __syncthreads();
             {
-                uint4 v = *reinterpret_cast<const uint4 *>(s_row + PER * tid);
                 uint16_t m[PER];
-                memcpy(m, &v, sizeof(v));
+#pragma unroll
+                for (int c = 0; c < PER; c += 8) {
+                    const uint4 v = *reinterpret_cast<const uint4 *>(s_row + PER * tid + c);
+                    memcpy(m + c, &v, sizeof(v));
+                }
                 uint32_t run = 0;
 #pragma unroll
                 for (int k = 0; k < PER; ++k) run = max(run, (uint32_t)m[k]);
@@ -137,8 +142,12 @@ __global__ void __launch_bounds__(ST, 6) k_stream(AccArgs a) {
                     run = max(run, (uint32_t)m[k]);
                     m[k] = (uint16_t)run;
                 }
-                memcpy(&v, m, sizeof(v));
-                *reinterpret_cast<uint4 *>(s_row + PER * tid) = v;
+#pragma unroll
+                for (int c = 0; c < PER; c += 8) {
+                    uint4 v;
+                    memcpy(&v, m + c, sizeof(v));
+                    *reinterpret_cast<uint4 *>(s_row + PER * tid + c) = v;
+                }
             }
             __syncthreads();
             for (uint64_t tb = b0 + tid; tb < b1; tb += (uint64_t)ST * SU) {
