@@ -26,8 +26,9 @@
 // most 4x wider per window); a window that overflows is cut at the
 // kHeavyCap-th touched column and the rest is taken by the next window.  The
 // symbolic pass (steps A, B and 1 on RW_SYM-wide windows: it keeps neither
-// accumulators nor the word prefix) counts each row's outputs as the columns
-// whose bit it set first.
+// accumulators nor the word prefix) marks with atomics whose result it does not
+// wait for and counts each window's columns by a popcount of its words, read
+// anyway to store and clear them.
 //
 // Kept bitmaps: for the heavy rows whose column bitmap over their rank span
 // costs at most kKeepBitsMax bits per product (kKeepBitsPerProduct when memory
@@ -590,7 +591,7 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
             const uint32_t nwu = rw >> 5;  // bitmap words in use
             uint32_t nextmin = INF;
             uint32_t ns = 0;
-            uint32_t newcols = 0;  // symbolic: columns this thread marked first
+            uint32_t newcols = 0;  // symbolic: columns in this thread's words of the window
             if (NUMERIC) {
                 // the region held the previous window's table (or a kept row's pairs): clear the bitmap
                 __syncthreads();
@@ -613,10 +614,7 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
                     [&](uint32_t, uint32_t, const RankItem &it) {
                         const uint32_t c = it.r - W0;
                         const uint32_t m = 1u << (c & 31);
-                        if (!(bits[c >> 5] & m)) {
-                            const uint32_t old = atomicOr(&bits[c >> 5], m);
-                            if (!NUMERIC) newcols += (old & m) ? 0u : 1u;
-                        }
+                        if (!(bits[c >> 5] & m)) atomicOr(&bits[c >> 5], m);  // no return value needed
                     });
                 __syncthreads();
             }
@@ -628,8 +626,9 @@ __global__ void __launch_bounds__(T, NUMERIC ? 2 : 3) k_rowwin(AccArgs a) {  // 
                 uint32_t *dst = nwr ? a.hbm + a.row_bmoff[row] : nullptr;
                 const uint32_t wo = nwr ? (W0 - s_rc.rb) >> 5 : 0u;  // a multiple of 4
                 for (uint32_t q = 4u * tid; q < nwu; q += 4u * T) {
-                    if (nwr && wo + q < nwr)
-                        *reinterpret_cast<uint4 *>(dst + wo + q) = *reinterpret_cast<const uint4 *>(bits + q);
+                    const uint4 v = *reinterpret_cast<const uint4 *>(bits + q);
+                    newcols += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+                    if (nwr && wo + q < nwr) *reinterpret_cast<uint4 *>(dst + wo + q) = v;
                     *reinterpret_cast<uint4 *>(bits + q) = make_uint4(0u, 0u, 0u, 0u);
                 }
                 // the window's new columns and the next window's start (the run
