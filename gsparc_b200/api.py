@@ -86,7 +86,7 @@ _lib = None
 
 EXPORTS = [
     "gsparc_version", "gsparc_status_string", "gsparc_last_error", "gsparc_ctx_create", "gsparc_ctx_reserve",
-    "gsparc_ctx_set_verify", "gsparc_ctx_set_tiles", "gsparc_ctx_set_row_bitmaps", "gsparc_host_pin",
+    "gsparc_ctx_set_verify", "gsparc_ctx_set_tiles", "gsparc_ctx_set_row_bitmaps", "gsparc_ctx_set_sort", "gsparc_host_pin",
     "gsparc_host_unpin",
     "gsparc_ctx_destroy", "gsparc_ctx_memory", "gsparc_tensor_upload", "gsparc_tensor_free",
     "gsparc_tensor_info", "gsparc_sptc", "gsparc_sptc_shard", "gsparc_read_tns", "gsparc_write_tns",
@@ -174,6 +174,7 @@ def lib():
     L.gsparc_ctx_set_verify.argtypes = [P, U64]
     L.gsparc_ctx_set_tiles.argtypes = [P, U64, ctypes.c_uint32]
     L.gsparc_ctx_set_row_bitmaps.argtypes = [P, I]
+    L.gsparc_ctx_set_sort.argtypes = [P, I]
     L.gsparc_host_pin.argtypes = [P, U64]
     L.gsparc_host_unpin.argtypes = [P]
     L.gsparc_ctx_destroy.argtypes = [P]
@@ -330,6 +331,11 @@ class Context:
         light_row_max products use the on-chip ESC (<= 2048), heavy windows hold
         at most heavy_window_cap outputs."""
         _check(lib().gsparc_ctx_set_tiles(self._h, light_row_max, heavy_window_cap), "ctx_set_tiles")
+
+    def set_sort(self, impl: int = 0):
+        """Sort of the operands' (key, value) pairs: 0 = CUB onesweep (default),
+        1 = this library's own stable radix sort; results are identical."""
+        _check(lib().gsparc_ctx_set_sort(self._h, impl), "ctx_set_sort")
 
     def set_row_bitmaps(self, on: bool = True):
         """Keep heavy rows' column bitmaps from the symbolic to the numeric pass

@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--ex
               "-I" + os.path.join(ROOT, "include"), "-I" + CSRC] + ARCH
 LIB_SOURCES = ["util.cpp", "prep.cu", "accumulate.cu", "rowwin.cu", "engine.cu", "capi.cpp", "tns_io.cpp",
                "noalloc.cu", "batch.cu", "stream.cu", "serve.cpp", "wide.cu", "chain.cu", "tune.cpp", "verify.cu",
-               "partition.cpp"]
+               "partition.cpp", "radix.cu"]
 CLI_SOURCES = ["cli.cpp"]
 
 

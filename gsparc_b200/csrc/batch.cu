@@ -759,8 +759,13 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
 
     // ---- sort ----
     int wx = 0, wy = 0;
-    sort_pairs(A, nx, xk0, xk1, xv0, xv1, kbx + jb, &wx, s);
-    sort_pairs(A, ny, yk0, yk1, yv0, yv1, kby + jb, &wy, s);
+    if (ctx->sort_impl) {  // gsparc_ctx_set_sort; a failed look-back sets bit 8 of the error word
+        own_sort_pairs(A, nx, xk0, xk1, xv0, xv1, kbx + jb, &wx, ctx->d_flag, s);
+        own_sort_pairs(A, ny, yk0, yk1, yv0, yv1, kby + jb, &wy, ctx->d_flag, s);
+    } else {
+        sort_pairs(A, nx, xk0, xk1, xv0, xv1, kbx + jb, &wx, s);
+        sort_pairs(A, ny, yk0, yk1, yv0, yv1, kby + jb, &wy, s);
+    }
     const uint64_t *xkeys = wx ? xk1.get() : xk0.get();
     const float *xvals = wx ? xv1.get() : xv0.get();
     const uint64_t *ykeys = wy ? yk1.get() : yk0.get();
@@ -1050,6 +1055,7 @@ void run_group(gsparc_ctx *ctx, std::vector<Job *> &G, uint64_t max_chunk_nnz, i
     GS_CUDA(cudaStreamSynchronize(s));
     bst.bytes_d2h += sizeof(JobOut) * (g + 1) + 64 + 4 * g + 8;
     GS_REQUIRE(!(herr & 2u), GSPARC_EINTERNAL, "light unit over capacity");
+    GS_REQUIRE(!(herr & 8u), GSPARC_EINTERNAL, "radix sort look-back gave up");
     const uint64_t ntot = jo[g].out_off;
     bst.nnz += ntot;
     mark(4);

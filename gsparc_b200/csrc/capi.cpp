@@ -141,6 +141,14 @@ gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint
     });
 }
 
+gsparc_status gsparc_ctx_set_sort(gsparc_ctx *ctx, int impl) {
+    return guard([&] {
+        GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
+        GS_REQUIRE(impl == 0 || impl == 1, GSPARC_EINVAL, "impl must be 0 (CUB) or 1 (this library's radix sort)");
+        ctx->sort_impl = impl;
+    });
+}
+
 gsparc_status gsparc_ctx_set_row_bitmaps(gsparc_ctx *ctx, int on) {
     return guard([&] {
         GS_REQUIRE(ctx, GSPARC_EINVAL, "null context");
@@ -467,12 +475,21 @@ gsparc_status gsparc_sort_pairs(gsparc_ctx *ctx, uint64_t n, uint64_t *d_keys, f
         gs::DBuf<uint64_t> k1(ctx->arena, n, s);
         gs::DBuf<float> v1(ctx->arena, n, s);
         int which = 0;
-        gs::sort_pairs(ctx->arena, n, d_keys, k1, d_vals, v1, nbits, &which, s);
+        unsigned int herr = 0;
+        if (ctx->sort_impl) {
+            gs::DBuf<unsigned int> err(ctx->arena, 1, s);
+            GS_CUDA(cudaMemsetAsync(err.get(), 0, 4, s));
+            gs::own_sort_pairs(ctx->arena, n, d_keys, k1, d_vals, v1, nbits, &which, err, s);
+            GS_CUDA(cudaMemcpyAsync(&herr, err.get(), 4, cudaMemcpyDeviceToHost, s));
+        } else {
+            gs::sort_pairs(ctx->arena, n, d_keys, k1, d_vals, v1, nbits, &which, s);
+        }
         if (which) {
             GS_CUDA(cudaMemcpyAsync(d_keys, k1.get(), 8 * n, cudaMemcpyDeviceToDevice, s));
             GS_CUDA(cudaMemcpyAsync(d_vals, v1.get(), 4 * n, cudaMemcpyDeviceToDevice, s));
         }
         GS_CUDA(cudaStreamSynchronize(s));
+        GS_REQUIRE(!herr, GSPARC_EINTERNAL, "radix sort look-back gave up");
     });
 }
 

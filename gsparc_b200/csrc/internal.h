@@ -151,6 +151,7 @@ struct gsparc_ctx {
     uint64_t light_row_max = 0;          // rows with at most this many products use the on-chip ESC (0: default)
     uint32_t heavy_window_cap = 0;       // heavy rows: outputs per window (0: the compiled capacity)
     int keep_row_bitmaps = 1;            // heavy rows: the symbolic pass keeps column bitmaps for the numeric pass
+    int sort_impl = 0;                   // operand sorts: 0 CUB onesweep, 1 this library's radix sort (radix.cu)
 };
 
 struct gsparc_tensor {

@@ -30,6 +30,11 @@ void sort_pairs(Arena &a, uint64_t n, uint64_t *keys0, uint64_t *keys1, float *v
                 int nbits, int *which, cudaStream_t s);
 void sort_keys(Arena &a, uint64_t n, uint64_t *keys0, uint64_t *keys1, int nbits, int *which,
                cudaStream_t s);
+// This library's own stable onesweep radix sort of the same pairs (radix.cu),
+// 8 bits per pass; same double-buffer contract as sort_pairs.  A look-back
+// wait that runs out sets bit 8 of *err (the caller's device error word).
+void own_sort_pairs(Arena &a, uint64_t n, uint64_t *keys0, uint64_t *keys1, float *vals0, float *vals1,
+                    int nbits, int *which, unsigned int *err, cudaStream_t s);
 
 // ---- Y preparation ----
 // From sorted Y keys (c << nfbits | f): per-entry column rank among the

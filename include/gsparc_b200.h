@@ -167,6 +167,13 @@ gsparc_status gsparc_ctx_set_tiles(gsparc_ctx *ctx, uint64_t light_row_max, uint
  * way.  No counterpart in the reference, whose ESC re-expands every product
  * (include/gsparc/contraction.cuh:440-561). */
 gsparc_status gsparc_ctx_set_row_bitmaps(gsparc_ctx *ctx, int on);
+/* Sort used for the operands' (key, value) pairs by later contractions and by
+ * gsparc_sort_pairs on this context: 0 = CUB's onesweep radix sort (the
+ * default; the reference sorts with CUB, include/gsparc/sort.cuh:90-108),
+ * 1 = this library's own stable LSD radix sort (8 bits per pass: a digit
+ * histogram per tile, a scan of the digit-major counts, a scatter ranked with
+ * warp match).  Both are stable, so results are identical either way. */
+gsparc_status gsparc_ctx_set_sort(gsparc_ctx *ctx, int impl);
 /* FP64 verification of every later contraction on this context: each output
  * chunk's values are compared, before delivery, with FP64 sums of their
  * matched products formed on the GPU, for all rows when a contraction has at
