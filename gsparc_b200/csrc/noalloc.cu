@@ -13,8 +13,8 @@
 //
 // The array's host-side name is only a stand-in; its device address is looked
 // up once per device with cudaGetSymbolAddress (with that device current) on
-// the first call made on that device, so that first call should come before
-// any stream capture.  `stream` must belong to the current device (checked).
+// the first call made on that device.  `stream` must belong to the current
+// device (checked).
 // Every call on a device shares the one array: calls whose work overlaps on
 // the GPU (different streams, or different host threads) race on it and must
 // be serialised by the caller.  No scratch content is carried from one call to

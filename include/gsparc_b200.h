@@ -487,9 +487,8 @@ gsparc_status gsparc_index_match(gsparc_ctx *ctx, uint64_t nx, const uint64_t *d
  * (Y up to roughly 4.9 million keys for small X); larger inputs return
  * GSPARC_EINVAL with the bytes needed in gsparc_last_error().  The first call
  * on each device looks the array's address up (cudaGetSymbolAddress) with
- * that device current, so that first call should come before any stream
- * capture.  `stream` must belong to the current device (GSPARC_EINVAL
- * otherwise).  With ir == NULL the call does not wait: the total stays in
+ * that device current.  `stream` must belong to the current device
+ * (GSPARC_EINVAL otherwise).  With ir == NULL the call does not wait: the total stays in
  * d_prefix[nx]; otherwise it waits for the stream and stores the total.
  * All calls on a device share the array, so calls that overlap on the GPU
  * race and must be serialised by the caller; nothing is carried over between
